@@ -1,0 +1,153 @@
+/*
+ * lnt.h - C ABI of the B200 sparse/dense multi-index-array (MIA) hot path.
+ *
+ * Plain pointers and sizes only.  Every array argument named *_keys / *_vals /
+ * A / B / C is DEVICE memory on the current CUDA device; every function is
+ * stream-ordered on `stream` (a cudaStream_t passed as void*, NULL = legacy
+ * default stream) and returns an lnt_status code for argument errors and
+ * launch failures.  Errors raised on the device (an expired bounded wait) are
+ * latched in a per-device word read back by lnt_device_status().
+ *
+ * Sparse storage is the reference's LCO layout (SparseMIA.h:61-84, 203-206):
+ * parallel arrays of 64-bit linear keys and float64 values, with
+ *     key = sum_i idx[seq[i]] * prod_{j<i} dims[seq[j]]     (first listed mode fastest)
+ * (IndexUtil.h:866-879).  Keys are unsigned here; the reference stores int64
+ * but only ever holds non-negative keys below the dimensionality.
+ *
+ * Caller-allocated workspaces: each entry point that needs scratch memory has
+ * a *_workspace() query giving the byte count; pass a device buffer at least
+ * that large (256-byte aligned).  No entry point allocates device memory.
+ */
+#ifndef LNT_H
+#define LNT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LNT_MAX_ORDER 16
+
+#if defined(__GNUC__)
+#define LNT_API __attribute__((visibility("default")))
+#else
+#define LNT_API
+#endif
+
+typedef enum lnt_status {
+    LNT_OK = 0,
+    LNT_BAD_ARG = 1,          /* null pointer, size out of range, misaligned workspace */
+    LNT_BAD_DIMS = 2,         /* dimension mismatch (reference: DimensionMismatchException) */
+    LNT_BAD_SEQ = 3,          /* a lexicographic sequence is not a permutation of 0..order-1 */
+    LNT_OVERFLOW_KEYBITS = 4, /* product of dims does not fit in 63 bits */
+    LNT_WORKSPACE = 5,        /* workspace smaller than the *_workspace() query */
+    LNT_TIMEOUT = 6,          /* a bounded device-side wait expired (device status only) */
+    LNT_DEVICE_ERROR = 7,     /* CUDA runtime error on launch */
+    LNT_UNSUPPORTED = 8       /* valid request outside what this build implements */
+} lnt_status;
+
+/* Re-keying request: keys linearised under cur_seq are re-linearised under
+ * new_seq.  order == 0 means "keys are used as they are". */
+typedef struct lnt_rekey_spec {
+    int32_t order;
+    int32_t cur_seq[LNT_MAX_ORDER];
+    int32_t new_seq[LNT_MAX_ORDER];
+    int64_t dims[LNT_MAX_ORDER];
+} lnt_rekey_spec;
+
+/* ---- library info / diagnostics ---------------------------------------- */
+
+/* Human-readable name of a status code. */
+LNT_API const char* lnt_status_string(int status);
+
+/* ABI version (major*10000 + minor*100 + patch). */
+LNT_API int lnt_version(void);
+
+/* Number of kernels this library has launched in the process so far. */
+LNT_API uint64_t lnt_launch_count(void);
+
+/* Reads (and, if clear != 0, resets) the device-side error word of the
+ * current device after synchronising `stream`.  Returns LNT_OK when no
+ * device-side wait expired since the last clear, else LNT_TIMEOUT.
+ * *detail (may be NULL) receives the raw word (which kernel gave up). */
+LNT_API int lnt_device_status(int clear, void* stream, uint32_t* detail);
+
+/* Per-kernel timing: while enabled, every launch by this library is
+ * bracketed by CUDA events on its own stream (a few microseconds of overhead
+ * per launch; off by default). */
+LNT_API int lnt_profile_enable(int on);
+/* Clears all timing records. */
+LNT_API int lnt_profile_reset(void);
+/* Synchronises the recorded events and returns, for kernels of the given name
+ * ("rekey", "sort_hist", "sort_onesweep", "sort_copy", "collect_lead",
+ * "collect", ...), the summed device time in milliseconds and the launch
+ * count since the last reset. */
+LNT_API int lnt_profile_query(const char* kernel, double* total_ms, uint64_t* launches);
+
+/* ---- key linearisation / permutation ----------------------------------- */
+
+/* Re-linearise n keys from cur_seq to new_seq over `dims` (order modes).
+ * keys_out may equal keys_in.  Replaces SparseMIABase::change_linIdx_sequence
+ * (SparseMIABase.h:768-814: create_shuffle_needs + reShuffleLinearIndex,
+ * IndexUtil.h:480-487, 567-589) and the mex gateway SparseChangeLinIdxMex
+ * (MATLAB/mex/sparse_change_linIdx.cpp:16-72; 0-based sequences here). */
+LNT_API int lnt_rekey(const uint64_t* keys_in, uint64_t* keys_out, size_t n, int order,
+              const int64_t* dims, const int32_t* cur_seq, const int32_t* new_seq,
+              void* stream);
+
+/* ---- sorting ------------------------------------------------------------ */
+
+/* Workspace bytes for lnt_sort_pairs on n pairs whose keys are < max_key. */
+LNT_API int lnt_sort_pairs_workspace(size_t n, uint64_t max_key, size_t* bytes);
+
+/* Ascending sort of (key, value) pairs by key; equal keys keep their input
+ * order (stable).  keys_out/vals_out may equal keys_in/vals_in (in-place).
+ * Only the ceil(log2(max_key)) low key bits are sorted, as the reference's
+ * radix sort does with its `max_size` argument.  Replaces SparseMIABase::sort()
+ * -> RadixSortInPlace_PowerOf2Radix_Unsigned (SparseMIABase.h:701-734,
+ * LibMIARadix.h:444-484) and SparseSortMex (MATLAB/mex/sparse_sort.cpp:14-60). */
+LNT_API int lnt_sort_pairs(const uint64_t* keys_in, const double* vals_in,
+                   uint64_t* keys_out, double* vals_out, size_t n, uint64_t max_key,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- duplicate collection ----------------------------------------------- */
+
+LNT_API int lnt_collect_duplicates_workspace(size_t n, size_t* bytes);
+
+/* Fold runs of equal keys of a key-sorted array with +.  With skip_zero_heads
+ * != 0 this is SparseMIA::collect_duplicates(std::plus) (SparseMIA.h:636-665):
+ * a run whose raw values are all exactly 0.0 is dropped unless it starts at
+ * position 0.  With skip_zero_heads == 0 it is collect_duplicates_function
+ * (FunctionUtil.h:701-728): every run is kept.  *d_nout (device) receives the
+ * output count.  Output buffers need room for n pairs and must not overlap
+ * the input. */
+LNT_API int lnt_collect_duplicates(const uint64_t* keys, const double* vals, size_t n,
+                           int skip_zero_heads, uint64_t* keys_out, double* vals_out,
+                           uint64_t* d_nout, void* workspace, size_t workspace_bytes,
+                           void* stream);
+
+/* ---- sort merge (both operands unsorted) -------------------------------- */
+
+LNT_API int lnt_sort_reduce_workspace(size_t na, size_t nb, uint64_t max_key, size_t* bytes);
+
+/* Concatenate A (re-keyed by a_rekey, may be NULL) and B (re-keyed by
+ * b_rekey, values multiplied by b_scale, +1 or -1), sort by key and collect
+ * duplicates (skip_zero_heads as in lnt_collect_duplicates).  This is
+ * SparseMIA::sortMerge (SparseMIA.h:833-887) for op = + (b_scale = 1) and
+ * op = - (b_scale = -1, the reference negates B while copying, :862-875);
+ * with nb == 0 it is change_linIdx_sequence + collect_duplicates.
+ * Output buffers need room for na+nb pairs; *d_nout (device) gets the count. */
+LNT_API int lnt_sort_reduce(const uint64_t* a_keys, const double* a_vals, size_t na,
+                    const lnt_rekey_spec* a_rekey,
+                    const uint64_t* b_keys, const double* b_vals, size_t nb,
+                    const lnt_rekey_spec* b_rekey, double b_scale,
+                    uint64_t max_key, int skip_zero_heads,
+                    uint64_t* keys_out, double* vals_out, uint64_t* d_nout,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LNT_H */

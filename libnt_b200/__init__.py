@@ -1,0 +1,238 @@
+"""libnt_b200 — B200 (sm_100a) implementation of the LibNT / LibMIA sparse and
+dense multi-index-array hot path.
+
+The product is the CUDA library ``liblnt_cuda.so`` (C ABI in ``include/lnt.h``)
+and the header-only C++ front end under ``libnt_b200/include/lnt/``.  This
+Python module is plumbing: it loads the library with ctypes and calls it on
+torch-allocated device buffers and torch's current CUDA stream.  There is no
+CPU fallback: if the library is missing, importing raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "liblnt_cuda.so"
+MAX_ORDER = 16
+
+STATUS = {
+    0: "ok", 1: "bad argument", 2: "dimension mismatch", 3: "sequence is not a permutation",
+    4: "dimensionality does not fit in 63 bits", 5: "workspace too small", 6: "device-side wait expired",
+    7: "CUDA error", 8: "unsupported request",
+}
+
+
+class LntError(RuntimeError):
+    """A non-zero lnt_status returned by the CUDA library."""
+
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: lnt status {status} ({STATUS.get(status, 'unknown')})")
+
+
+class RekeySpec(C.Structure):
+    """lnt_rekey_spec (include/lnt.h)."""
+    _fields_ = [("order", C.c_int32), ("cur_seq", C.c_int32 * MAX_ORDER), ("new_seq", C.c_int32 * MAX_ORDER),
+                ("dims", C.c_int64 * MAX_ORDER)]
+
+    @classmethod
+    def make(cls, dims, cur_seq, new_seq) -> "RekeySpec":
+        s = cls()
+        s.order = len(dims)
+        for i, (d, c, n) in enumerate(zip(dims, cur_seq, new_seq)):
+            s.dims[i], s.cur_seq[i], s.new_seq[i] = int(d), int(c), int(n)
+        return s
+
+
+_vp = C.c_void_p
+_sz = C.c_size_t
+_SIGS = {
+    "lnt_status_string": ([C.c_int], C.c_char_p),
+    "lnt_version": ([], C.c_int),
+    "lnt_launch_count": ([], C.c_uint64),
+    "lnt_device_status": ([C.c_int, _vp, C.POINTER(C.c_uint32)], C.c_int),
+    "lnt_profile_enable": ([C.c_int], C.c_int),
+    "lnt_profile_reset": ([], C.c_int),
+    "lnt_profile_query": ([C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)], C.c_int),
+    "lnt_rekey": ([_vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp], C.c_int),
+    "lnt_sort_pairs_workspace": ([_sz, C.c_uint64, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_sort_pairs": ([_vp, _vp, _vp, _vp, _sz, C.c_uint64, _vp, _sz, _vp], C.c_int),
+    "lnt_collect_duplicates_workspace": ([_sz, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_collect_duplicates": ([_vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
+    "lnt_sort_reduce_workspace": ([_sz, _sz, C.c_uint64, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_sort_reduce": ([_vp, _vp, _sz, C.POINTER(RekeySpec), _vp, _vp, _sz, C.POINTER(RekeySpec), C.c_double,
+                         C.c_uint64, C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m libnt_b200.build` "
+                              "(there is no CPU fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def _check(st: int, what: str):
+    if st != 0:
+        raise LntError(st, what)
+
+
+# ---------------------------------------------------------------------------
+# torch plumbing
+# ---------------------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream():
+    return _vp(_torch().cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return _vp(t.data_ptr()) if t is not None else None
+
+
+def _dev(t):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t
+
+
+def workspace(nbytes: int, device=None):
+    torch = _torch()
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device or "cuda")
+
+
+def _arr(vals, dtype):
+    return (dtype * len(vals))(*[int(v) for v in vals])
+
+
+def launch_count() -> int:
+    return int(lib().lnt_launch_count())
+
+
+def device_status(clear: bool = True) -> int:
+    word = C.c_uint32(0)
+    st = lib().lnt_device_status(int(clear), _stream(), C.byref(word))
+    if st not in (0, 6):
+        _check(st, "lnt_device_status")
+    return int(word.value)
+
+
+def profile_enable(on: bool = True):
+    _check(lib().lnt_profile_enable(int(bool(on))), "lnt_profile_enable")
+
+
+def profile_reset():
+    _check(lib().lnt_profile_reset(), "lnt_profile_reset")
+
+
+def profile_query(kernel: str):
+    """(total device ms, launches) of a kernel since the last reset."""
+    t = C.c_double(0)
+    n = C.c_uint64(0)
+    _check(lib().lnt_profile_query(kernel.encode(), C.byref(t), C.byref(n)), "lnt_profile_query")
+    return t.value, int(n.value)
+
+
+def rekey(keys, dims, cur_seq, new_seq, out=None):
+    """Re-linearise int64/uint64 keys (device tensor) from cur_seq to new_seq."""
+    torch = _torch()
+    _dev(keys)
+    out = torch.empty_like(keys) if out is None else _dev(out)
+    n = len(dims)
+    st = lib().lnt_rekey(_ptr(keys), _ptr(out), keys.numel(), n, _arr(dims, C.c_int64), _arr(cur_seq, C.c_int32),
+                         _arr(new_seq, C.c_int32), _stream())
+    _check(st, "lnt_rekey")
+    return out
+
+
+def sort_pairs(keys, vals, max_key: int, out_keys=None, out_vals=None):
+    """Stable ascending sort by key; returns (keys, vals) (new tensors unless given)."""
+    torch = _torch()
+    _dev(keys), _dev(vals)
+    n = keys.numel()
+    ok = torch.empty_like(keys) if out_keys is None else out_keys
+    ov = torch.empty_like(vals) if out_vals is None else out_vals
+    nb = C.c_size_t(0)
+    _check(lib().lnt_sort_pairs_workspace(n, int(max_key), C.byref(nb)), "lnt_sort_pairs_workspace")
+    ws = workspace(nb.value, keys.device)
+    st = lib().lnt_sort_pairs(_ptr(keys), _ptr(vals), _ptr(ok), _ptr(ov), n, int(max_key), _ptr(ws), nb.value,
+                              _stream())
+    _check(st, "lnt_sort_pairs")
+    return ok, ov
+
+
+def collect_duplicates(keys, vals, skip_zero_heads: bool = True):
+    """Fold equal-key runs of key-sorted pairs; returns trimmed (keys, vals)."""
+    torch = _torch()
+    _dev(keys), _dev(vals)
+    n = keys.numel()
+    ok = torch.empty_like(keys)
+    ov = torch.empty_like(vals)
+    cnt = torch.zeros(1, dtype=torch.int64, device=keys.device)
+    nb = C.c_size_t(0)
+    _check(lib().lnt_collect_duplicates_workspace(n, C.byref(nb)), "lnt_collect_duplicates_workspace")
+    ws = workspace(nb.value, keys.device)
+    st = lib().lnt_collect_duplicates(_ptr(keys), _ptr(vals), n, int(bool(skip_zero_heads)), _ptr(ok), _ptr(ov),
+                                      _ptr(cnt), _ptr(ws), nb.value, _stream())
+    _check(st, "lnt_collect_duplicates")
+    m = int(cnt.item())
+    return ok[:m], ov[:m]
+
+
+def sort_reduce_workspace(na: int, nb: int, max_key: int) -> int:
+    b = C.c_size_t(0)
+    _check(lib().lnt_sort_reduce_workspace(na, nb, int(max_key), C.byref(b)), "lnt_sort_reduce_workspace")
+    return b.value
+
+
+def sort_reduce(a_keys, a_vals, b_keys=None, b_vals=None, *, max_key: int, a_rekey: RekeySpec | None = None,
+                b_rekey: RekeySpec | None = None, b_scale: float = 1.0, skip_zero_heads: bool = True,
+                out_keys=None, out_vals=None, count=None, ws=None, sync: bool = True):
+    """Concatenate A and B (each optionally re-keyed, B scaled), sort and
+    collect duplicates.  With sync=True returns trimmed (keys, vals); else
+    returns (keys, vals, count_tensor) without synchronising."""
+    torch = _torch()
+    _dev(a_keys), _dev(a_vals)
+    na = a_keys.numel()
+    nb = b_keys.numel() if b_keys is not None else 0
+    n = na + nb
+    ok = torch.empty(n, dtype=a_keys.dtype, device=a_keys.device) if out_keys is None else out_keys
+    ov = torch.empty(n, dtype=a_vals.dtype, device=a_vals.device) if out_vals is None else out_vals
+    cnt = torch.zeros(1, dtype=torch.int64, device=a_keys.device) if count is None else count
+    need = sort_reduce_workspace(na, nb, max_key)
+    if ws is None or ws.numel() < need:
+        ws = workspace(need, a_keys.device)
+    st = lib().lnt_sort_reduce(_ptr(a_keys), _ptr(a_vals), na, C.byref(a_rekey) if a_rekey else None,
+                               _ptr(b_keys), _ptr(b_vals), nb, C.byref(b_rekey) if b_rekey else None,
+                               float(b_scale), int(max_key), int(bool(skip_zero_heads)), _ptr(ok), _ptr(ov),
+                               _ptr(cnt), _ptr(ws), ws.numel(), _stream())
+    _check(st, "lnt_sort_reduce")
+    if not sync:
+        return ok, ov, cnt
+    m = int(cnt.item())
+    return ok[:m], ov[:m]

@@ -1,0 +1,357 @@
+// Duplicate collection on key-sorted pairs (segmented sum + compaction) and
+// the fused sort-merge entry point.
+//
+// collect: two kernels over tiles of 2048 pairs.
+//   lead_kernel   - one warp per tile sums the tile's leading run (the
+//                   elements before the tile's first new key) so a run that
+//                   crosses tiles is finished from per-tile summaries instead
+//                   of element by element.
+//   collect_kernel- stages the tile in shared memory, lets the thread that
+//                   holds a run's first element sum the run, counts the runs
+//                   kept, takes its output offset by decoupled look-back and
+//                   writes (key, sum) pairs contiguously.
+// Traffic: 16 B read per input pair + 16 B written per output pair.
+#include <algorithm>
+
+#include "lnt_sort.cuh"
+
+namespace lnt {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kItems = 8;
+constexpr int kTile = kThreads * kItems;  // 2048
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagPre = 2ull << 62;
+constexpr unsigned long long kFlagMask = 3ull << 62;
+constexpr unsigned long long kValMask = (1ull << 62) - 1ull;
+
+struct LeadSummary {
+  double sum;     // sum of the tile's leading run
+  u32 anynz;      // some value in the leading run is non-zero
+  u32 full;       // the whole tile is one leading run (no new key inside)
+};
+
+__global__ void __launch_bounds__(128) lead_kernel(const u64* __restrict__ keys, const double* __restrict__ vals,
+                                                   size_t n, u32 ntiles, LeadSummary* __restrict__ lead) {
+  const int lane = threadIdx.x & 31;
+  const u32 tile = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (tile >= ntiles) return;
+  const size_t base = (size_t)tile * kTile;
+  const size_t end = min(n, base + kTile);
+  LeadSummary r{0.0, 0u, 0u};
+  if (base == 0) {  // tile 0 has no leading run (position 0 starts a run)
+    if (lane == 0) lead[tile] = r;
+    return;
+  }
+  const u64 prev = keys[base - 1];
+  double sum = 0.0;
+  bool anynz = false;
+  bool stop = false;
+  for (size_t c = base; c < end; c += 32) {
+    const size_t i = c + lane;
+    const bool brk = (i < end) && keys[i] != prev;
+    const u32 m = __ballot_sync(0xffffffffu, brk);  // lanes where a new key starts
+    const int nvalid = (int)min((size_t)32, end - c);
+    const int upto = m ? (__ffs(m) - 1) : nvalid;  // warp-uniform
+    const double v = (lane < upto) ? vals[i] : 0.0;
+    // sequential summation in index order (every lane holds the same sum)
+    for (int l = 0; l < upto; ++l) {
+      double x = __shfl_sync(0xffffffffu, v, l);
+      sum += x;
+      anynz |= (x != 0.0);
+    }
+    if (m) {
+      stop = true;
+      break;
+    }
+  }
+  if (lane == 0) {
+    r.sum = sum;
+    r.anynz = anynz ? 1u : 0u;
+    r.full = stop ? 0u : 1u;
+    lead[tile] = r;
+  }
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile64(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ void st_volatile64(unsigned long long* p, unsigned long long v) {
+  *reinterpret_cast<volatile unsigned long long*>(p) = v;
+}
+
+__global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict__ keys,
+                                                           const double* __restrict__ vals, size_t n,
+                                                           u32 ntiles, int skip_zero_heads,
+                                                           const LeadSummary* __restrict__ lead,
+                                                           unsigned long long* __restrict__ status,
+                                                           u32* __restrict__ tile_counter,
+                                                           u64* __restrict__ out_k, double* __restrict__ out_v,
+                                                           u64* __restrict__ d_nout) {
+  __shared__ u64 s_k[kTile + 1];
+  __shared__ double s_v[kTile];
+  __shared__ u32 s_warp[kThreads / 32];
+  __shared__ u32 s_tile;
+  __shared__ unsigned long long s_off;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  const u32 tile = s_tile;
+  const size_t base = (size_t)tile * kTile;
+  const u32 tn = (u32)min((size_t)kTile, n - base);
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    u32 idx = j * kThreads + tid;
+    if (idx < tn) {
+      s_k[idx + 1] = __ldcs(keys + base + idx);
+      s_v[idx] = __ldcs(vals + base + idx);
+    }
+  }
+  if (tid == 0) s_k[0] = base ? keys[base - 1] : 0ull;
+  __syncthreads();
+
+  // ---- runs that start in this thread's items -----------------------------
+  u64 rk[kItems];
+  double rs[kItems];
+  u32 kept_mask = 0;
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    u32 idx = tid * kItems + j;
+    rk[j] = 0;
+    rs[j] = 0.0;
+    if (idx >= tn) continue;
+    const size_t gi = base + idx;
+    const u64 k = s_k[idx + 1];
+    const bool head = (gi == 0) || (k != s_k[idx]);
+    if (!head) continue;
+    double sum = s_v[idx];
+    bool anynz = sum != 0.0;
+    u32 m = idx + 1;
+    while (m < tn && s_k[m + 1] == k) {
+      double x = s_v[m];
+      sum += x;
+      anynz |= (x != 0.0);
+      ++m;
+    }
+    if (m == tn) {  // the run may continue into later tiles
+      for (u32 u = tile + 1; u < ntiles; ++u) {
+        LeadSummary L = lead[u];
+        sum += L.sum;
+        anynz |= (L.anynz != 0u);
+        if (!L.full) break;
+      }
+    }
+    const bool kept = !skip_zero_heads || gi == 0 || anynz;
+    if (kept) {
+      kept_mask |= 1u << j;
+      rk[j] = k;
+      rs[j] = sum;
+    }
+  }
+
+  // ---- block scan of kept counts -----------------------------------------
+  const u32 local = __popc(kept_mask);
+  u32 inc = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    u32 t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  u32 excl = inc - local;
+  u32 total = 0;
+  for (int w = 0; w < kThreads / 32; ++w) {
+    if (w < warp) excl += s_warp[w];
+    total += s_warp[w];
+  }
+
+  // ---- look-back for the tile's output offset -----------------------------
+  if (tid == 0) {
+    unsigned long long off = 0;
+    if (tile == 0) {
+      st_volatile64(&status[0], kFlagPre | total);
+    } else {
+      st_volatile64(&status[tile], kFlagAgg | total);
+      int p = (int)tile - 1;
+      u32 spins = 0;
+      while (p >= 0) {
+        unsigned long long w = ld_volatile64(&status[p]);
+        unsigned long long f = w & kFlagMask;
+        if (f == 0) {
+          if (++spins > kSpinLimit) {
+            latch_error(kErrReduceLookback);
+            break;
+          }
+          continue;
+        }
+        off += w & kValMask;
+        if (f == kFlagPre) break;
+        --p;
+      }
+      st_volatile64(&status[tile], kFlagPre | (off + total));
+    }
+    s_off = off;
+    if (tile == ntiles - 1) *d_nout = off + total;
+  }
+  __syncthreads();  // everyone is done reading s_k / s_v
+
+  // ---- stage results contiguously, then write coalesced -------------------
+  u32 r = excl;
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    if (kept_mask & (1u << j)) {
+      s_k[r] = rk[j];
+      s_v[r] = rs[j];
+      ++r;
+    }
+  }
+  __syncthreads();
+  const unsigned long long off = s_off;
+  for (u32 i = tid; i < total; i += kThreads) {
+    __stcs(out_k + off + i, s_k[i]);
+    __stcs(out_v + off + i, s_v[i]);
+  }
+}
+
+}  // namespace
+
+struct CollectLayout {
+  u32 ntiles;
+  size_t off_lead, off_status, off_counter, total;
+};
+
+static CollectLayout collect_layout(size_t n) {
+  CollectLayout L;
+  L.ntiles = (u32)((n + kTile - 1) / kTile);
+  size_t off = 0;
+  L.off_lead = off;
+  off += align_up((size_t)L.ntiles * sizeof(LeadSummary), 256);
+  L.off_status = off;
+  off += align_up((size_t)L.ntiles * 8, 256);
+  L.off_counter = off;
+  off += 256;
+  L.total = off;
+  return L;
+}
+
+size_t collect_workspace_bytes(size_t n) { return collect_layout(n).total; }
+
+int run_collect(const u64* keys, const double* vals, size_t n, int skip_zero_heads, u64* out_k,
+                double* out_v, u64* d_nout, void* ws, cudaStream_t s) {
+  if (n == 0) {
+    return cudaMemsetAsync(d_nout, 0, sizeof(u64), s) == cudaSuccess ? LNT_OK : LNT_DEVICE_ERROR;
+  }
+  CollectLayout L = collect_layout(n);
+  unsigned char* w = static_cast<unsigned char*>(ws);
+  // status + counter are contiguous: one memset
+  if (cudaMemsetAsync(w + L.off_status, 0, L.total - L.off_status, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  LeadSummary* lead = reinterpret_cast<LeadSummary*>(w + L.off_lead);
+  {
+    ProfScope prof("collect_lead", s);
+    lead_kernel<<<(L.ntiles + 3) / 4, 128, 0, s>>>(keys, vals, n, L.ntiles, lead);
+  }
+  ProfScope prof("collect", s);
+  collect_kernel<<<L.ntiles, kThreads, 0, s>>>(keys, vals, n, L.ntiles, skip_zero_heads, lead,
+                                               reinterpret_cast<unsigned long long*>(w + L.off_status),
+                                               reinterpret_cast<u32*>(w + L.off_counter), out_k, out_v, d_nout);
+  count_launch(2);
+  return launch_status();
+}
+
+}  // namespace lnt
+
+using namespace lnt;
+
+namespace {
+struct SortReduceLayout {
+  SortPlan plan;
+  size_t off_ctrl, off_k0, off_v0, off_k1, off_v1, off_coll, total;
+};
+
+SortReduceLayout sort_reduce_layout(size_t n, u64 max_key) {
+  SortReduceLayout L;
+  L.plan = make_sort_plan(n, max_key, choose_sort_bits(n, key_bits_for(max_key)));
+  size_t off = 0;
+  L.off_ctrl = off;
+  off += align_up(L.plan.ctrl_bytes, 256);
+  L.off_k0 = off;
+  off += align_up(n * 8, 256);
+  L.off_v0 = off;
+  off += align_up(n * 8, 256);
+  L.off_k1 = off;
+  off += align_up(n * 8, 256);
+  L.off_v1 = off;
+  off += align_up(n * 8, 256);
+  L.off_coll = off;
+  off += align_up(collect_workspace_bytes(n), 256);
+  L.total = off;
+  return L;
+}
+}  // namespace
+
+extern "C" {
+
+int lnt_collect_duplicates_workspace(size_t n, size_t* bytes) {
+  if (!bytes) return LNT_BAD_ARG;
+  *bytes = collect_workspace_bytes(n);
+  return LNT_OK;
+}
+
+int lnt_collect_duplicates(const uint64_t* keys, const double* vals, size_t n, int skip_zero_heads,
+                           uint64_t* keys_out, double* vals_out, uint64_t* d_nout, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  if (!d_nout) return LNT_BAD_ARG;
+  if (n && (!keys || !vals || !keys_out || !vals_out)) return LNT_BAD_ARG;
+  if (n && (!workspace || workspace_bytes < collect_workspace_bytes(n))) return LNT_WORKSPACE;
+  return run_collect((const u64*)keys, vals, n, skip_zero_heads, (u64*)keys_out, vals_out, (u64*)d_nout,
+                     workspace, as_stream(stream));
+}
+
+int lnt_sort_reduce_workspace(size_t na, size_t nb, uint64_t max_key, size_t* bytes) {
+  if (!bytes) return LNT_BAD_ARG;
+  if (na + nb >= (1u << 30)) return LNT_UNSUPPORTED;
+  *bytes = sort_reduce_layout(na + nb, max_key).total;
+  return LNT_OK;
+}
+
+int lnt_sort_reduce(const uint64_t* a_keys, const double* a_vals, size_t na, const lnt_rekey_spec* a_rekey,
+                    const uint64_t* b_keys, const double* b_vals, size_t nb, const lnt_rekey_spec* b_rekey,
+                    double b_scale, uint64_t max_key, int skip_zero_heads, uint64_t* keys_out,
+                    double* vals_out, uint64_t* d_nout, void* workspace, size_t workspace_bytes,
+                    void* stream) {
+  const size_t n = na + nb;
+  if (!d_nout) return LNT_BAD_ARG;
+  if ((na && (!a_keys || !a_vals)) || (nb && (!b_keys || !b_vals))) return LNT_BAD_ARG;
+  if (n && (!keys_out || !vals_out)) return LNT_BAD_ARG;
+  if (n >= (1u << 30)) return LNT_UNSUPPORTED;
+  cudaStream_t s = as_stream(stream);
+  if (n == 0) return run_collect(nullptr, nullptr, 0, skip_zero_heads, nullptr, nullptr, (u64*)d_nout, nullptr, s);
+  SortReduceLayout L = sort_reduce_layout(n, max_key);
+  if (!workspace || workspace_bytes < L.total) return LNT_WORKSPACE;
+  if ((uintptr_t)workspace % 256) return LNT_BAD_ARG;
+  PairSource src;
+  src.ak = (const u64*)a_keys;
+  src.av = a_vals;
+  src.na = na;
+  src.bk = (const u64*)b_keys;
+  src.bv = b_vals;
+  src.nb = nb;
+  src.bscale = b_scale;
+  src.pad = 0;
+  int st = make_rekey_params(a_rekey, &src.ra);
+  if (st != LNT_OK) return st;
+  st = make_rekey_params(b_rekey, &src.rb);
+  if (st != LNT_OK) return st;
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  u64* k0 = reinterpret_cast<u64*>(w + L.off_k0);
+  double* v0 = reinterpret_cast<double*>(w + L.off_v0);
+  u64* k1 = reinterpret_cast<u64*>(w + L.off_k1);
+  double* v1 = reinterpret_cast<double*>(w + L.off_v1);
+  st = run_sort(L.plan, src, k0, v0, k1, v1, w + L.off_ctrl, s);
+  if (st != LNT_OK) return st;
+  return run_collect(k0, v0, n, skip_zero_heads, (u64*)keys_out, vals_out, (u64*)d_nout, w + L.off_coll, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,239 @@
+"""Pins the oracle (CPU restatement) against the reference: its own compiled
+kernels (oracle/_ref, when the reference tree was present at build time),
+its golden fixtures and its known-answer / property tests.  CPU only."""
+import itertools
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference kernels not compiled (no reference tree)")
+
+
+# ---------------------------------------------------------------------------
+# against the reference's own compiled kernels
+# ---------------------------------------------------------------------------
+
+@needs_ref
+@pytest.mark.parametrize("order", [2, 3, 4, 5, 6, 8])
+def test_rekey_matches_reference_kernel(order, rng):
+    for trial in range(4):
+        dims = [int(x) for x in rng.integers(1, 40 if order < 6 else 9, order)]
+        total = int(np.prod(dims))
+        keys = rng.integers(0, total, 5000, dtype=np.uint64)
+        cur = list(rng.permutation(order))
+        new = list(rng.permutation(order))
+        np.testing.assert_array_equal(oracle.rekey(keys, dims, cur, new), oracle.ref_rekey(keys, dims, cur, new))
+
+
+@needs_ref
+def test_rekey_512_4_reversal_matches_reference():
+    rng = np.random.default_rng(1)
+    dims = [512] * 4
+    keys = rng.integers(0, 2 ** 36, 200000, dtype=np.uint64)
+    got = oracle.rekey(keys, dims, [0, 1, 2, 3], [3, 2, 1, 0])
+    np.testing.assert_array_equal(got, oracle.ref_rekey(keys, dims, [0, 1, 2, 3], [3, 2, 1, 0]))
+
+
+def _multiset_equal_per_key(k1, v1, k2, v2):
+    """keys identical; values equal as a multiset within each key run."""
+    np.testing.assert_array_equal(k1, k2)
+    o1 = np.lexsort((v1, k1))
+    o2 = np.lexsort((v2, k2))
+    np.testing.assert_array_equal(v1[o1], v2[o2])
+
+
+@needs_ref
+@pytest.mark.parametrize("n,bits", [(0, 8), (1, 8), (49, 10), (50, 10), (2999, 20), (3000, 20), (3001, 36),
+                                    (100000, 36), (250000, 22), (70000, 11), (70000, 12)])
+def test_sort_matches_reference_radix(n, bits, rng):
+    keys = rng.integers(0, 2 ** bits, n, dtype=np.uint64)
+    if n > 10:
+        keys[: n // 10] = keys[n // 3]  # heavy duplicates
+    vals = rng.standard_normal(n)
+    k_ref, v_ref = oracle.ref_radix_sort(keys, vals, 2 ** bits)
+    k, v = oracle.sort_pairs(keys, vals)
+    assert np.all(k[1:] >= k[:-1])
+    _multiset_equal_per_key(k, v, k_ref, v_ref)
+
+
+@needs_ref
+def test_introsort_matches_reference(rng):
+    keys = rng.integers(0, 1000, 2500, dtype=np.uint64)
+    vals = rng.standard_normal(2500)
+    k_ref, v_ref = oracle.ref_introsort(keys, vals)
+    k, v = oracle.sort_pairs(keys, vals)
+    _multiset_equal_per_key(k, v, k_ref, v_ref)
+
+
+# ---------------------------------------------------------------------------
+# the reference's golden fixtures and KATs
+# ---------------------------------------------------------------------------
+
+def test_dense_golden_fixture_bit_exact():
+    """DenseLattice data/test1.bin x test2.bin == multtest_ddd.bin
+    (denselatticemulttests.cpp:19-49)."""
+    z = np.load(GOLDEN / "dense_lattice_5x5x10.npz")
+    h, w, wB, d = (int(x) for x in z["shape"])
+    np.testing.assert_array_equal(oracle.dense_lattice_mult(z["A"], z["B"], h, w, wB, d), z["C"])
+
+
+def test_dense_closed_form_kat():
+    """dense_mia_mult_test.cpp:44-74: a increments 1..dim2^2 along the inner
+    modes, b = 1, so every c = dim2^2 (dim2^2 + 1) / 2."""
+    dim1, dim2 = 3, 4
+    h, w, wB = dim1 * dim1, dim2 * dim2, dim1 * dim1
+    # lattice A: rows (i,k), cols (j,l) with value incrementing over (j,l)
+    A = np.empty((h, w))
+    A[:, :] = np.arange(1, w + 1)[None, :]
+    B = np.ones((w, wB))
+    Cm = oracle.dense_lattice_mult(A.ravel(order="F"), B.ravel(order="F"), h, w, wB, 1)
+    assert np.all(Cm == w * (w + 1) / 2)
+
+
+def test_collect_duplicates_plus_kat(rng):
+    """sparse_mia_functions.cpp:66-92: keys {2,1} then random 1/2 keys with
+    value 1; collecting with + gives the two counts."""
+    n = 40
+    keys = np.empty(n, np.uint64)
+    vals = np.ones(n)
+    keys[0], keys[1] = 2, 1
+    coin = rng.random(n - 2) >= 0.5
+    keys[2:] = np.where(coin, 1, 2)
+    c1 = 1 + int(coin.sum())
+    c2 = 1 + int((~coin).sum())
+    k, v = oracle.sort_pairs(keys, vals)
+    k, v = oracle.collect_duplicates(k, v)
+    np.testing.assert_array_equal(k, [1, 2])
+    np.testing.assert_array_equal(v, [c1, c2])
+
+
+def test_collect_duplicates_zero_quirk():
+    """SparseMIA.h:645-655: a run starting with exact zeros starts at its first
+    non-zero; all-zero runs vanish except the one at position 0; cancelled
+    sums stay."""
+    keys = np.array([1, 1, 3, 3, 3, 5, 7, 7, 9], np.uint64)
+    vals = np.array([0.0, 0.0, 0.0, 2.0, 0.0, 0.0, 1.5, -1.5, -0.0])
+    k, v = oracle.collect_duplicates(keys, vals, skip_zero_heads=True)
+    np.testing.assert_array_equal(k, [1, 3, 7])
+    np.testing.assert_array_equal(v, [0.0, 2.0, 0.0])
+    k, v = oracle.collect_duplicates(keys, vals, skip_zero_heads=False)
+    np.testing.assert_array_equal(k, [1, 3, 5, 7, 9])
+    np.testing.assert_array_equal(v, [0.0, 2.0, 0.0, 0.0, -0.0])
+
+
+@pytest.mark.parametrize("seq", [[2, 0, 3, 1], [1, 2, 3, 0], [0, 1, 2, 3], [2, 3, 0, 1]])
+def test_sort_seq_equals_rekey_then_sort(seq, rng):
+    """sparse_mia_functions.cpp:101-215: sort(seq) on sorted data equals
+    change_linIdx_sequence(seq) followed by sort(), element by element."""
+    dims = [3, 3, 3, 3]
+    total = int(np.prod(dims))
+    m = oracle.SparseMIA(dims, rng.integers(0, total, total // 2, dtype=np.uint64), rng.uniform(-5, 5, total // 2),
+                         sorted=False)
+    m.collect_duplicates()
+    m2 = m.copy()
+    m.sort(seq)
+    m2.change_linIdx_sequence(seq)
+    m2.sort()
+    np.testing.assert_array_equal(m.keys, m2.keys)
+    np.testing.assert_array_equal(m.vals, m2.vals)
+
+
+# ---------------------------------------------------------------------------
+# differential tests (sparse vs dense), as the reference's suites do
+# ---------------------------------------------------------------------------
+
+def _random_sparse(rng, dims, density=0.3, ones=False, seq=None, sorted_=False):
+    total = int(np.prod(dims))
+    dense = rng.uniform(0, 20, dims)
+    dense[dense < 20 * (1 - density)] = 0  # reference: randu(0,20), threshold
+    if ones:
+        dense[dense != 0] = 1.0
+    nz = np.flatnonzero(dense.ravel(order="F"))
+    m = oracle.SparseMIA(list(dims), nz.astype(np.uint64), dense.ravel(order="F")[nz], sorted=True)
+    if seq is not None:
+        m.change_linIdx_sequence(seq)
+        if sorted_:
+            m.sort()
+    return m, dense
+
+
+@pytest.mark.parametrize("a_state,b_state", list(itertools.product(["unsorted", "sorted", "sorted_other"], repeat=2)))
+@pytest.mark.parametrize("op", [0, 1])
+def test_merge_branches_match_dense(a_state, b_state, op, rng):
+    """sparse_mia_add_sub_tests.cpp:23-488 pattern: c(i,j,k,l) = a(i,j,k,l) +/- b(l,k,j,i)
+    through the scan and the sort merge branches, against dense arithmetic."""
+    dims = [5, 8, 5, 8]
+    bd = [dims[3], dims[2], dims[1], dims[0]]
+    a, da = _random_sparse(rng, dims)
+    b, db = _random_sparse(rng, bd)
+    for m, st in ((a, a_state), (b, b_state)):
+        if st == "unsorted":
+            m.change_linIdx_sequence([2, 0, 3, 1])
+        elif st == "sorted_other":
+            m.sort([1, 3, 0, 2])
+    order = oracle.merge_index_order(list("ijkl"), list("lkji"))
+    assert order == [3, 2, 1, 0]
+    c = oracle.merge(a, b, order, op)
+    expect = da + (1 if op == 0 else -1) * db.transpose(3, 2, 1, 0)
+    np.testing.assert_allclose(c.to_dense(), expect, rtol=0, atol=1e-12)
+    # the result is key-sorted under its own sequence
+    assert np.all(c.keys[1:] > c.keys[:-1])
+
+
+def test_sort_merge_sequence_rule():
+    """sortMerge with |A| == |B| re-keys A to B's order: the result carries
+    linIdxSequence {3,2,1,0} for c(i,j,k,l)=a(i,j,k,l)+b(l,k,j,i)."""
+    rng = np.random.default_rng(3)
+    dims = [4, 5, 6, 7]
+    a = oracle.SparseMIA(dims, rng.integers(0, 840, 50, dtype=np.uint64), rng.standard_normal(50), sorted=False)
+    b = oracle.SparseMIA(dims[::-1], rng.integers(0, 840, 50, dtype=np.uint64), rng.standard_normal(50),
+                         sorted=False)
+    c = oracle.merge(a, b, [3, 2, 1, 0])
+    assert c.seq == [3, 2, 1, 0] and c.sorted
+    # |A| > |B|: B is re-keyed into A's order, C keeps A's default sequence
+    a2 = oracle.SparseMIA(dims, rng.integers(0, 840, 60, dtype=np.uint64), rng.standard_normal(60), sorted=False)
+    b2 = oracle.SparseMIA(dims[::-1], rng.integers(0, 840, 50, dtype=np.uint64), rng.standard_normal(50),
+                          sorted=False)
+    c2 = oracle.merge(a2, b2, [3, 2, 1, 0])
+    assert c2.seq == [0, 1, 2, 3] and b2.seq == [3, 2, 1, 0] and not b2.sorted
+
+
+@pytest.mark.parametrize("a_lab,b_lab", [("ijk", "klj"), ("ijk", "jkl"), ("ij", "jk"), ("ikj", "jlk")])
+def test_product_matches_dense(a_lab, b_lab, rng):
+    """sparse_mia_mult_test.cpp:19-168 pattern: sparse product vs dense einsum."""
+    dimmap = {"i": 8, "j": 5, "k": 6, "l": 7}
+    a, da = _random_sparse(rng, [dimmap[c] for c in a_lab])
+    b, db = _random_sparse(rng, [dimmap[c] for c in b_lab])
+    c, c_lab = oracle.product(a, list(a_lab), b, list(b_lab))
+    expect = np.einsum(f"{a_lab},{b_lab}->{''.join(c_lab)}", da, db)
+    np.testing.assert_allclose(c.to_dense(), expect, rtol=0, atol=1e-10)
+    assert np.all(c.keys[1:] > c.keys[:-1])
+
+
+def test_product_with_elementwise_index(rng):
+    """Inter (element-wise '!') index becomes the tab: c(i,l,n) = a(i,j,!n) * b(j,l,!n)."""
+    a, da = _random_sparse(rng, [6, 5, 4])
+    b, db = _random_sparse(rng, [5, 7, 4])
+    c, lab = oracle.product(a, ["i", "j", "!n"], b, ["j", "l", "!n"])
+    assert lab == ["i", "l", "!n"]
+    np.testing.assert_allclose(c.to_dense(), np.einsum("ijn,jln->iln", da, db), atol=1e-10)
+
+
+def test_lattice_mult_cross_check_dense(rng):
+    """csc_no_accum restatement vs a dense per-tab product on hypersparse
+    lattices (sparse_lattice_mult_test_specialized.cpp:16-88 cross-checks)."""
+    h, w, wB, d = 30, 40, 20, 5
+    for density in (0.01, 0.1, 0.5):
+        A = np.where(rng.random((h, w, d)) < density, rng.standard_normal((h, w, d)), 0.0)
+        B = np.where(rng.random((w, wB, d)) < density, rng.standard_normal((w, wB, d)), 0.0)
+        ak = np.flatnonzero(A.ravel(order="F")).astype(np.uint64)
+        bk = np.flatnonzero(B.ravel(order="F")).astype(np.uint64)
+        ck, cv = oracle.lattice_mult(ak, A.ravel(order="F")[ak.astype(np.int64)], h, w, d, bk,
+                                     B.ravel(order="F")[bk.astype(np.int64)], wB)
+        Cd = np.zeros(h * wB * d)
+        Cd[ck.astype(np.int64)] = cv
+        np.testing.assert_allclose(Cd, np.einsum("rkt,kct->rct", A, B).ravel(order="F"), atol=1e-12)
