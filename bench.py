@@ -228,7 +228,7 @@ def run_ours(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
-    na = nb = NNZ
+    na = nb = 1 << args.nnz_log2
     ak = torch.randint(0, MAX_KEY, (na,), generator=g, device=dev, dtype=torch.int64)
     bk = torch.randint(0, MAX_KEY, (nb,), generator=g, device=dev, dtype=torch.int64)
     av = torch.rand(na, generator=g, device=dev, dtype=torch.float64) * 2 - 1
@@ -278,6 +278,12 @@ def run_ours(args):
     L.profile_reset()
     n_out = int(cnt.item())
     assert L.device_status() == 0, "device-side wait expired during timing"
+
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "nnz/s", "ms_per_step": ms,
+                              "nnz_per_operand": na, "kernels": kernels}), flush=True)
+        return 0
 
     # ---- end-to-end through the C ABI from pinned host buffers ------------
     hk_a = ak.cpu().pin_memory()
@@ -364,6 +370,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--nnz-log2", type=int, default=26,
+                    help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
+    ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -112,6 +112,13 @@ LNT_API int lnt_sort_pairs(const uint64_t* keys_in, const double* vals_in,
                    uint64_t* keys_out, double* vals_out, size_t n, uint64_t max_key,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* Kernel variants of the sort compiled into this library (digit width, CTA
+ * threads, keys per thread, look-back window); the autotuner times each one.
+ * The variant used is the tuned choice, or LNT_SORT_VARIANT=<index> from the
+ * environment. */
+LNT_API int lnt_sort_variant_count(void);
+LNT_API int lnt_sort_variant(int index, int* bits, int* threads, int* items, int* window);
+
 /* ---- duplicate collection ----------------------------------------------- */
 
 LNT_API int lnt_collect_duplicates_workspace(size_t n, size_t* bytes);

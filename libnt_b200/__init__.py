@@ -58,6 +58,8 @@ _SIGS = {
     "lnt_profile_reset": ([], C.c_int),
     "lnt_profile_query": ([C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)], C.c_int),
     "lnt_rekey": ([_vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp], C.c_int),
+    "lnt_sort_variant_count": ([], C.c_int),
+    "lnt_sort_variant": ([C.c_int] + [C.POINTER(C.c_int)] * 4, C.c_int),
     "lnt_sort_pairs_workspace": ([_sz, C.c_uint64, C.POINTER(C.c_size_t)], C.c_int),
     "lnt_sort_pairs": ([_vp, _vp, _vp, _vp, _sz, C.c_uint64, _vp, _sz, _vp], C.c_int),
     "lnt_collect_duplicates_workspace": ([_sz, C.POINTER(C.c_size_t)], C.c_int),
@@ -170,17 +172,23 @@ def rekey(keys, dims, cur_seq, new_seq, out=None):
     return out
 
 
-def sort_pairs(keys, vals, max_key: int, out_keys=None, out_vals=None):
+def sort_pairs_workspace(n: int, max_key: int) -> int:
+    nb = C.c_size_t(0)
+    _check(lib().lnt_sort_pairs_workspace(n, int(max_key), C.byref(nb)), "lnt_sort_pairs_workspace")
+    return nb.value
+
+
+def sort_pairs(keys, vals, max_key: int, out_keys=None, out_vals=None, ws=None):
     """Stable ascending sort by key; returns (keys, vals) (new tensors unless given)."""
     torch = _torch()
     _dev(keys), _dev(vals)
     n = keys.numel()
     ok = torch.empty_like(keys) if out_keys is None else out_keys
     ov = torch.empty_like(vals) if out_vals is None else out_vals
-    nb = C.c_size_t(0)
-    _check(lib().lnt_sort_pairs_workspace(n, int(max_key), C.byref(nb)), "lnt_sort_pairs_workspace")
-    ws = workspace(nb.value, keys.device)
-    st = lib().lnt_sort_pairs(_ptr(keys), _ptr(vals), _ptr(ok), _ptr(ov), n, int(max_key), _ptr(ws), nb.value,
+    need = sort_pairs_workspace(n, max_key)
+    if ws is None or ws.numel() < need:
+        ws = workspace(need, keys.device)
+    st = lib().lnt_sort_pairs(_ptr(keys), _ptr(vals), _ptr(ok), _ptr(ov), n, int(max_key), _ptr(ws), ws.numel(),
                               _stream())
     _check(st, "lnt_sort_pairs")
     return ok, ov

@@ -81,6 +81,43 @@ __device__ __forceinline__ void st_volatile64(unsigned long long* p, unsigned lo
   *reinterpret_cast<volatile unsigned long long*>(p) = v;
 }
 
+// Shared-memory slot of tile element i (+1 for the predecessor key at slot 0),
+// padded by one word per 8 so blocked (stride-8) reads are conflict-free.
+__device__ __forceinline__ u32 pk(u32 i) { return i + (i >> 3); }
+constexpr u32 kPadded = kTile + 1 + (kTile + 1) / 8 + 1;
+
+// Warp-cooperative decoupled look-back over single-value tile states:
+// lane q reads the state of tile (base - q); one round trip covers 32
+// predecessors.  Returns the exclusive prefix of `tile` (all lanes).
+__device__ __forceinline__ unsigned long long warp_lookback(const unsigned long long* status, u32 tile, u32 err) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long excl = 0;
+  int base = (int)tile - 1;
+  u32 spins = 0;
+  while (base >= 0) {
+    const int p = base - lane;
+    const unsigned long long w = p >= 0 ? *reinterpret_cast<const volatile unsigned long long*>(status + p)
+                                        : kFlagPre;
+    const unsigned long long f = w & kFlagMask;
+    const u32 notready = __ballot_sync(0xffffffffu, f == 0);
+    const u32 pre = __ballot_sync(0xffffffffu, f == kFlagPre);
+    const int first_nr = notready ? __ffs(notready) - 1 : 32;
+    const int first_pre = pre ? __ffs(pre) - 1 : 32;
+    const int take = first_pre < first_nr ? first_pre + 1 : first_nr;  // lanes [0, take) contribute
+    unsigned long long v = lane < take ? (w & kValMask) : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    excl += v;
+    if (first_pre < first_nr) break;
+    base -= first_nr;
+    if (first_nr < 32 && ++spins > kSpinLimit) {
+      latch_error(err);
+      break;
+    }
+  }
+  return excl;
+}
+
 __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict__ keys,
                                                            const double* __restrict__ vals, size_t n,
                                                            u32 ntiles, int skip_zero_heads,
@@ -89,8 +126,8 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
                                                            u32* __restrict__ tile_counter,
                                                            u64* __restrict__ out_k, double* __restrict__ out_v,
                                                            u64* __restrict__ d_nout) {
-  __shared__ u64 s_k[kTile + 1];
-  __shared__ double s_v[kTile];
+  __shared__ u64 s_k[kPadded];
+  __shared__ double s_v[kPadded];
   __shared__ u32 s_warp[kThreads / 32];
   __shared__ u32 s_tile;
   __shared__ unsigned long long s_off;
@@ -104,8 +141,8 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
   for (int j = 0; j < kItems; ++j) {
     u32 idx = j * kThreads + tid;
     if (idx < tn) {
-      s_k[idx + 1] = __ldcs(keys + base + idx);
-      s_v[idx] = __ldcs(vals + base + idx);
+      s_k[pk(idx + 1)] = __ldcs(keys + base + idx);
+      s_v[pk(idx)] = __ldcs(vals + base + idx);
     }
   }
   if (tid == 0) s_k[0] = base ? keys[base - 1] : 0ull;
@@ -122,14 +159,14 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
     rs[j] = 0.0;
     if (idx >= tn) continue;
     const size_t gi = base + idx;
-    const u64 k = s_k[idx + 1];
-    const bool head = (gi == 0) || (k != s_k[idx]);
+    const u64 k = s_k[pk(idx + 1)];
+    const bool head = (gi == 0) || (k != s_k[pk(idx)]);
     if (!head) continue;
-    double sum = s_v[idx];
+    double sum = s_v[pk(idx)];
     bool anynz = sum != 0.0;
     u32 m = idx + 1;
-    while (m < tn && s_k[m + 1] == k) {
-      double x = s_v[m];
+    while (m < tn && s_k[pk(m + 1)] == k) {
+      double x = s_v[pk(m)];
       sum += x;
       anynz |= (x != 0.0);
       ++m;
@@ -167,33 +204,16 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
     total += s_warp[w];
   }
 
-  // ---- look-back for the tile's output offset -----------------------------
-  if (tid == 0) {
-    unsigned long long off = 0;
-    if (tile == 0) {
-      st_volatile64(&status[0], kFlagPre | total);
-    } else {
-      st_volatile64(&status[tile], kFlagAgg | total);
-      int p = (int)tile - 1;
-      u32 spins = 0;
-      while (p >= 0) {
-        unsigned long long w = ld_volatile64(&status[p]);
-        unsigned long long f = w & kFlagMask;
-        if (f == 0) {
-          if (++spins > kSpinLimit) {
-            latch_error(kErrReduceLookback);
-            break;
-          }
-          continue;
-        }
-        off += w & kValMask;
-        if (f == kFlagPre) break;
-        --p;
-      }
-      st_volatile64(&status[tile], kFlagPre | (off + total));
+  // ---- look-back for the tile's output offset (warp 0) --------------------
+  if (warp == 0) {
+    if (lane == 0)
+      st_volatile64(&status[tile], (tile == 0 ? kFlagPre : kFlagAgg) | total);
+    unsigned long long off = tile == 0 ? 0ull : warp_lookback(status, tile, kErrReduceLookback);
+    if (lane == 0) {
+      if (tile != 0) st_volatile64(&status[tile], kFlagPre | (off + total));
+      s_off = off;
+      if (tile == ntiles - 1) *d_nout = off + total;
     }
-    s_off = off;
-    if (tile == ntiles - 1) *d_nout = off + total;
   }
   __syncthreads();  // everyone is done reading s_k / s_v
 
@@ -272,7 +292,7 @@ struct SortReduceLayout {
 
 SortReduceLayout sort_reduce_layout(size_t n, u64 max_key) {
   SortReduceLayout L;
-  L.plan = make_sort_plan(n, max_key, choose_sort_bits(n, key_bits_for(max_key)));
+  L.plan = make_sort_plan(n, max_key);
   size_t off = 0;
   L.off_ctrl = off;
   off += align_up(L.plan.ctrl_bytes, 256);

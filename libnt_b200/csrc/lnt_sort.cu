@@ -5,6 +5,7 @@
 // reference's sort is unstable, so no order among equal keys is promised
 // there).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "lnt_sort.cuh"
@@ -12,7 +13,7 @@
 namespace lnt {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;  // histogram kernel CTA size
 constexpr int kWarps = kThreads / 32;
 constexpr u32 kFlagAgg = 1u << 30;
 constexpr u32 kFlagPre = 2u << 30;
@@ -54,13 +55,27 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const PairSource src, u3
   for (int i = threadIdx.x; i < passes * RADIX; i += kThreads) sh_hist[i] = 0;
   __syncthreads();
   const u32 stride = gridDim.x * kThreads;
-  for (u32 i = blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+  constexpr int U = 8;  // independent loads in flight per thread
+  u32 i = blockIdx.x * kThreads + threadIdx.x;
+  for (; i + (U - 1) * stride < n; i += U * stride) {
+    u64 k[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) k[u] = load_key<true>(src, i + u * stride);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      for (int p = 0; p < passes; ++p) {
+        const int shift = p * BITS;
+        const int w = min(BITS, key_bits - shift);
+        atomicAdd(&sh_hist[p * RADIX + ((u32)(k[u] >> shift) & ((1u << w) - 1u))], 1u);
+      }
+    }
+  }
+  for (; i < n; i += stride) {
     u64 k = load_key<true>(src, i);
     for (int p = 0; p < passes; ++p) {
-      int shift = p * BITS;
-      int w = min(BITS, key_bits - shift);
-      u32 d = (u32)(k >> shift) & ((1u << w) - 1u);
-      atomicAdd(&sh_hist[p * RADIX + d], 1u);
+      const int shift = p * BITS;
+      const int w = min(BITS, key_bits - shift);
+      atomicAdd(&sh_hist[p * RADIX + ((u32)(k >> shift) & ((1u << w) - 1u))], 1u);
     }
   }
   __syncthreads();
@@ -111,32 +126,65 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const PairSource src, u3
 // ---------------------------------------------------------------------------
 // One digit pass.
 // ---------------------------------------------------------------------------
-template <int BITS, int ITEMS>
-struct OnesweepSmem {
+template <int BITS, int THREADS, int ITEMS>
+struct OnesweepShape {
   static constexpr int RADIX = 1 << BITS;
-  static constexpr int TILE = kThreads * ITEMS;
-  static constexpr size_t bytes = (size_t)TILE * 8 + (size_t)kWarps * RADIX * 4 + (size_t)RADIX * 8 + 64;
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr int TILE = THREADS * ITEMS;
+  static constexpr int DPT = (RADIX + THREADS - 1) / THREADS;  // digits per thread
+  static constexpr size_t smem = (size_t)TILE * 16 + (size_t)WARPS * RADIX * 4 + (size_t)RADIX * 8 + 64;
+  // CTAs per SM that shared memory allows (228 KB per SM, 1 KB reserved per CTA), at most 4
+  static constexpr int kFit = (int)((228u * 1024u) / (smem + 1024u));
+  static constexpr int MINB = kFit < 1 ? 1 : (kFit > 4 ? 4 : kFit);
 };
 
-template <int BITS, int ITEMS, bool FIRST>
-__global__ void __launch_bounds__(kThreads) onesweep_kernel(const PairSource src, u64* __restrict__ out_k,
-                                                            double* __restrict__ out_v, u32 n, u32 shift,
-                                                            u32 mask, const u32* __restrict__ bstart,
-                                                            u32* __restrict__ status,
-                                                            u32* __restrict__ tile_counter) {
-  constexpr int RADIX = 1 << BITS;
-  constexpr int TILE = kThreads * ITEMS;
-  constexpr int DPT = (RADIX + kThreads - 1) / kThreads;  // digits per thread
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <bool FIRST>
+__device__ __forceinline__ const double* val_ptr(const PairSource& s, size_t i) {
+  if (!FIRST || i < s.na) return s.av + i;
+  return s.bv + (i - s.na);
+}
+
+// Lanes of the warp holding the same BITS-bit digit (one ballot per bit).
+template <int BITS>
+__device__ __forceinline__ u32 match_digit(u32 d) {
+  u32 peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    const u32 bit = (d >> b) & 1u;
+    const u32 m = __ballot_sync(0xffffffffu, bit);
+    peers &= bit ? m : ~m;
+  }
+  return peers;
+}
+
+template <int BITS, int THREADS, int ITEMS, int W, bool FIRST>
+__global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>::MINB))
+    onesweep_kernel(const PairSource src, u64* __restrict__ out_k, double* __restrict__ out_v, u32 n, u32 shift,
+                    u32 mask, const u32* __restrict__ bstart, u32* __restrict__ status,
+                    u32* __restrict__ tile_counter) {
+  using S = OnesweepShape<BITS, THREADS, ITEMS>;
+  constexpr int RADIX = S::RADIX;
+  constexpr int WARPS = S::WARPS;
+  constexpr int TILE = S::TILE;
+  constexpr int DPT = S::DPT;
   extern __shared__ __align__(16) unsigned char smem[];
-  u64* s_x = reinterpret_cast<u64*>(smem);                         // TILE
-  u32* s_whist = reinterpret_cast<u32*>(s_x + TILE);               // kWarps * RADIX
-  u32* s_tstart = s_whist + kWarps * RADIX;                        // RADIX
-  u32* s_glob = s_tstart + RADIX;                                  // RADIX
-  u32* s_misc = s_glob + RADIX;                                    // 16
+  u64* s_x = reinterpret_cast<u64*>(smem);               // TILE: tile in digit order
+  double* s_v = reinterpret_cast<double*>(s_x + TILE);   // TILE: values in input order
+  u32* s_whist = reinterpret_cast<u32*>(s_v + TILE);     // WARPS * RADIX
+  u32* s_tstart = s_whist + WARPS * RADIX;               // RADIX
+  u32* s_glob = s_tstart + RADIX;                        // RADIX
+  u32* s_misc = s_glob + RADIX;                          // 16
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_misc[0] = atomicAdd(tile_counter, 1u);
-  for (int i = tid; i < kWarps * RADIX; i += kThreads) s_whist[i] = 0;
+  for (int i = tid; i < WARPS * RADIX; i += THREADS) s_whist[i] = 0;
   __syncthreads();
   const u32 tile = s_misc[0];
   const size_t tile_base = (size_t)tile * TILE;
@@ -147,52 +195,49 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(const PairSource src
   u64 key[ITEMS];
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    u32 off = warp_base + i * 32 + lane;
-    key[i] = off < tile_n ? load_key<FIRST>(src, tile_base + off) : ~0ull;
+    const u32 off = warp_base + i * 32 + lane;
+    key[i] = off < tile_n ? load_key<FIRST>(src, tile_base + off) : 0ull;
   }
-
-  // ---- stable rank within (warp, digit) ----------------------------------
-  u32 pos[ITEMS];
-  const u32 lt_mask = (1u << lane) - 1u;
+  // values go straight to shared memory; the copy overlaps everything up to
+  // the value scatter and holds no registers
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    u32 off = warp_base + i * 32 + lane;
-    u32 d = off < tile_n ? ((u32)(key[i] >> shift) & mask) : (u32)RADIX;
-    u32 peers = __match_any_sync(0xffffffffu, d);
-    int leader = __ffs(peers) - 1;
-    u32 base = 0;
-    if (lane == leader && d < (u32)RADIX) base = atomicAdd(&s_whist[warp * RADIX + d], (u32)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    pos[i] = base + __popc(peers & lt_mask);
+    const u32 off = warp_base + i * 32 + lane;
+    if (off < tile_n) cp_async8(&s_v[off], val_ptr<FIRST>(src, tile_base + off));
+  }
+  cp_async_commit();
+
+  // ---- per-warp digit counts (no return values: fire-and-forget) ---------
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const u32 off = warp_base + i * 32 + lane;
+    if (off < tile_n) atomicAdd(&s_whist[warp * RADIX + ((u32)(key[i] >> shift) & mask)], 1u);
   }
   __syncthreads();
 
-  // ---- per digit: scan over warps, publish tile aggregate ----------------
+  // ---- tile counts: publish at once so successors can look back ----------
   u32 cnt[DPT];
   u32 local = 0;
 #pragma unroll
   for (int j = 0; j < DPT; ++j) {
-    int d = tid * DPT + j;
-    u32 sum = 0;
+    const int d = tid * DPT + j;
+    u32 c = 0;
     if (d < RADIX) {
 #pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        u32 c = s_whist[w * RADIX + d];
-        s_whist[w * RADIX + d] = sum;
-        sum += c;
-      }
-      u32 word = tile == 0 ? (kFlagPre | (bstart[d] + sum)) : (kFlagAgg | sum);
+      for (int w = 0; w < WARPS; ++w) c += s_whist[w * RADIX + d];
+      const u32 word = tile == 0 ? (kFlagPre | (bstart[d] + c)) : (kFlagAgg | c);
       st_volatile(&status[(size_t)tile * RADIX + d], word);
     }
-    cnt[j] = sum;
-    local += sum;
+    cnt[j] = c;
+    local += c;
   }
-  // ---- block exclusive scan of digit counts -> tile-local digit starts ----
+  // ---- block exclusive scan of digit counts; per-(warp, digit) bases ------
+  u32 tstart[DPT];
   {
     u32 inc = local;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      u32 t = __shfl_up_sync(0xffffffffu, inc, o);
+      const u32 t = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= o) inc += t;
     }
     if (lane == 31) s_misc[4 + warp] = inc;
@@ -201,60 +246,106 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(const PairSource src
     for (int w = 0; w < warp; ++w) run += s_misc[4 + w];
 #pragma unroll
     for (int j = 0; j < DPT; ++j) {
-      int d = tid * DPT + j;
-      if (d < RADIX) s_tstart[d] = run;
+      const int d = tid * DPT + j;
+      tstart[j] = run;
+      if (d < RADIX) {
+        u32 b = run;
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) {
+          const u32 c = s_whist[w * RADIX + d];
+          s_whist[w * RADIX + d] = b;
+          b += c;
+        }
+      }
       run += cnt[j];
+    }
+  }
+
+  // ---- decoupled look-back, W predecessors per round trip per digit -------
+  {
+    u32 excl[DPT];
+    int p[DPT];
+    bool done[DPT];
+#pragma unroll
+    for (int j = 0; j < DPT; ++j) {
+      const int d = tid * DPT + j;
+      excl[j] = (tile == 0 && d < RADIX) ? bstart[d] : 0u;
+      p[j] = (int)tile - 1;
+      done[j] = (d >= RADIX) || tile == 0;
+    }
+    u32 spins = 0;
+    while (true) {
+      bool all_done = true;
+#pragma unroll
+      for (int j = 0; j < DPT; ++j) all_done = all_done && done[j];
+      if (all_done) break;
+      u32 w[DPT][W];
+#pragma unroll
+      for (int j = 0; j < DPT; ++j) {
+        const int d = tid * DPT + j;
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          const int pp = p[j] - q;
+          w[j][q] = (!done[j] && pp >= 0) ? ld_volatile(&status[(size_t)pp * RADIX + d]) : kFlagPre;
+        }
+      }
+      bool stalled = false;
+#pragma unroll
+      for (int j = 0; j < DPT; ++j) {
+        if (done[j]) continue;
+        int q = 0;
+#pragma unroll
+        for (; q < W; ++q) {
+          const u32 f = w[j][q] & kFlagMask;
+          if (f == 0) break;
+          excl[j] += w[j][q] & kValMask;
+          if (f == kFlagPre) {
+            done[j] = true;
+            break;
+          }
+        }
+        if (!done[j]) {
+          p[j] -= q;
+          if (q < W) stalled = true;
+        }
+      }
+      if (stalled && ++spins > kSpinLimit) {
+        latch_error(kErrSortLookback);
+        break;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < DPT; ++j) {
+      const int d = tid * DPT + j;
+      if (d >= RADIX) break;
+      if (tile != 0) st_volatile(&status[(size_t)tile * RADIX + d], kFlagPre | (excl[j] + cnt[j]));
+      s_glob[d] = excl[j] - tstart[j];
     }
   }
   __syncthreads();
 
-  // ---- tile positions; stage keys in digit order --------------------------
+  // ---- stable rank: ballot match + per-(warp, digit) running base ---------
+  u32 pos[ITEMS];
+  const u32 lt_mask = (1u << lane) - 1u;
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    u32 off = warp_base + i * 32 + lane;
-    if (off < tile_n) {
-      u32 d = (u32)(key[i] >> shift) & mask;
-      pos[i] += s_tstart[d] + s_whist[warp * RADIX + d];
-      s_x[pos[i]] = key[i];
-    }
+    const u32 off = warp_base + i * 32 + lane;
+    const bool valid = off < tile_n;
+    const u32 vmask = __ballot_sync(0xffffffffu, valid);
+    const u32 d = valid ? ((u32)(key[i] >> shift) & mask) : 0u;
+    const u32 peers = match_digit<BITS>(d) & vmask;
+    u32 base = 0;
+    if (valid) base = s_whist[warp * RADIX + d];
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) s_whist[warp * RADIX + d] = base + __popc(peers);
+    __syncwarp();
+    pos[i] = base + __popc(peers & lt_mask);
   }
-  // values are fetched now so their latency overlaps the look-back
-  double val[ITEMS];
+  // ---- stage keys in digit order ------------------------------------------
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
-    u32 off = warp_base + i * 32 + lane;
-    val[i] = off < tile_n ? load_val<FIRST>(src, tile_base + off) : 0.0;
-  }
-
-  // ---- decoupled look-back per digit ---------------------------------------
-#pragma unroll
-  for (int j = 0; j < DPT; ++j) {
-    int d = tid * DPT + j;
-    if (d >= RADIX) break;
-    u32 excl;
-    if (tile == 0) {
-      excl = bstart[d];
-    } else {
-      excl = 0;
-      int p = (int)tile - 1;
-      u32 spins = 0;
-      while (p >= 0) {
-        u32 w = ld_volatile(&status[(size_t)p * RADIX + d]);
-        u32 f = w & kFlagMask;
-        if (f == 0) {
-          if (++spins > kSpinLimit) {
-            latch_error(kErrSortLookback);
-            break;
-          }
-          continue;
-        }
-        excl += w & kValMask;
-        if (f == kFlagPre) break;
-        --p;
-      }
-      st_volatile(&status[(size_t)tile * RADIX + d], kFlagPre | (excl + cnt[j]));
-    }
-    s_glob[d] = excl - s_tstart[d];
+    const u32 off = warp_base + i * 32 + lane;
+    if (off < tile_n) s_x[pos[i]] = key[i];
   }
   __syncthreads();
 
@@ -262,40 +353,63 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(const PairSource src
   u32 dst[ITEMS];
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
-    u32 idx = j * kThreads + tid;
+    const u32 idx = j * THREADS + tid;
     if (idx < tile_n) {
-      u64 k = s_x[idx];
-      u32 d = (u32)(k >> shift) & mask;
-      dst[j] = s_glob[d] + idx;
+      const u64 k = s_x[idx];
+      dst[j] = s_glob[(u32)(k >> shift) & mask] + idx;
       __stcs(out_k + dst[j], k);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const u32 off = warp_base + i * 32 + lane;
+    if (off < tile_n) {
+      double v = s_v[off];
+      if (FIRST && tile_base + off >= src.na) v *= src.bscale;
+      reinterpret_cast<double*>(s_x)[pos[i]] = v;
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < ITEMS; ++i) {
-    u32 off = warp_base + i * 32 + lane;
-    if (off < tile_n) reinterpret_cast<double*>(s_x)[pos[i]] = val[i];
-  }
-  __syncthreads();
-#pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
-    u32 idx = j * kThreads + tid;
+    const u32 idx = j * THREADS + tid;
     if (idx < tile_n) __stcs(out_v + dst[j], reinterpret_cast<const double*>(s_x)[idx]);
   }
 }
 
-template <int BITS>
-constexpr int items_for_bits() {
-  return BITS <= 8 ? 16 : (BITS <= 10 ? 12 : 8);
+// Copies the (possibly re-keyed / concatenated) source into buf0 unchanged;
+// used when there is nothing to sort (all keys equal).
+__global__ void copy_source_kernel(const PairSource src, u64* __restrict__ ok, double* __restrict__ ov, u32 n) {
+  const u32 stride = gridDim.x * blockDim.x;
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    ok[i] = load_key<true>(src, i);
+    ov[i] = load_val<true>(src, i);
+  }
 }
 
-template <int BITS>
-int run_sort_bits(const SortPlan& plan, const PairSource& src, u64* buf0_k, double* buf0_v,
-                  u64* buf1_k, double* buf1_v, void* ctrl, cudaStream_t s) {
-  constexpr int RADIX = 1 << BITS;
-  constexpr int ITEMS = items_for_bits<BITS>();
-  constexpr int TILE = kThreads * ITEMS;
-  if (plan.ntiles != (plan.n + TILE - 1) / TILE) return LNT_BAD_ARG;
+// Compiled variants: (digit bits, CTA threads, items per thread, look-back window).
+#define LNT_SORT_VARIANTS(X) \
+  X(8, 256, 16, 16)          \
+  X(8, 256, 16, 32)          \
+  X(8, 512, 8, 16)           \
+  X(8, 384, 12, 16)          \
+  X(8, 256, 12, 16)          \
+  X(9, 512, 8, 16)           \
+  X(9, 512, 8, 32)           \
+  X(9, 256, 12, 8)
+
+#define LNT_SV_ENTRY(B, T, I, W) {B, T, I, W},
+const SortVariant kVariants[] = {LNT_SORT_VARIANTS(LNT_SV_ENTRY)};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+template <int BITS, int THREADS, int ITEMS, int W>
+int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, double* buf0_v, u64* buf1_k,
+                     double* buf1_v, void* ctrl, cudaStream_t s) {
+  using Sh = OnesweepShape<BITS, THREADS, ITEMS>;
+  constexpr int RADIX = Sh::RADIX;
+  if (plan.tile != (u32)Sh::TILE || plan.bits != BITS) return LNT_BAD_ARG;
   unsigned char* c = static_cast<unsigned char*>(ctrl);
   u32* ghist = reinterpret_cast<u32*>(c + plan.off_ghist);
   u32* bstart = reinterpret_cast<u32*>(c + plan.off_bstart);
@@ -305,36 +419,39 @@ int run_sort_bits(const SortPlan& plan, const PairSource& src, u64* buf0_k, doub
 
   // histogram of all passes
   {
-    size_t sh = (size_t)plan.passes * RADIX * 4;
+    const size_t sh = (size_t)plan.passes * RADIX * 4;
     auto kern = hist_kernel<BITS>;
     if (sh > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-    int blocks = std::max(1, std::min((int)((plan.n + kThreads * 16 - 1) / (kThreads * 16)), sm_count() * 4));
+    const int blocks =
+        std::max(1, std::min((int)((plan.n + kThreads * 16 - 1) / (kThreads * 16)), sm_count() * 4));
     ProfScope prof("sort_hist", s);
     kern<<<blocks, kThreads, sh, s>>>(src, plan.n, plan.passes, plan.key_bits, ghist, bstart,
                                       counters + plan.passes);
     count_launch();
   }
-  constexpr size_t sh = OnesweepSmem<BITS, ITEMS>::bytes;
+  constexpr size_t sh = Sh::smem;
   // (function attributes are per device: set them on every call)
-  cudaFuncSetAttribute(onesweep_kernel<BITS, ITEMS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-  cudaFuncSetAttribute(onesweep_kernel<BITS, ITEMS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  cudaFuncSetAttribute(onesweep_kernel<BITS, THREADS, ITEMS, W, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  cudaFuncSetAttribute(onesweep_kernel<BITS, THREADS, ITEMS, W, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   const u64* in_k = nullptr;
   const double* in_v = nullptr;
   for (int p = 0; p < plan.passes; ++p) {
-    int which = (plan.passes - 1 - p) & 1;
+    const int which = (plan.passes - 1 - p) & 1;
     u64* ok = which ? buf1_k : buf0_k;
     double* ov = which ? buf1_v : buf0_v;
-    int shift = p * BITS;
-    int w = std::min(BITS, plan.key_bits - shift);
-    u32 mask = (1u << w) - 1u;
+    const int shift = p * BITS;
+    const int w = std::min(BITS, plan.key_bits - shift);
+    const u32 mask = (1u << w) - 1u;
     u32* st = status + (size_t)p * plan.ntiles * RADIX;
     ProfScope prof("sort_onesweep", s);
     if (p == 0) {
-      onesweep_kernel<BITS, ITEMS, true><<<plan.ntiles, kThreads, sh, s>>>(
+      onesweep_kernel<BITS, THREADS, ITEMS, W, true><<<plan.ntiles, THREADS, sh, s>>>(
           src, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
     } else {
-      PairSource ps = plain_source(in_k, in_v, plan.n);
-      onesweep_kernel<BITS, ITEMS, false><<<plan.ntiles, kThreads, sh, s>>>(
+      const PairSource ps = plain_source(in_k, in_v, plan.n);
+      onesweep_kernel<BITS, THREADS, ITEMS, W, false><<<plan.ntiles, THREADS, sh, s>>>(
           ps, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
     }
     count_launch();
@@ -344,43 +461,50 @@ int run_sort_bits(const SortPlan& plan, const PairSource& src, u64* buf0_k, doub
   return launch_status();
 }
 
-// Copies the (possibly re-keyed / concatenated) source into buf0 unchanged;
-// used when there is nothing to sort (all keys equal).
-__global__ void copy_source_kernel(const PairSource src, u64* __restrict__ ok, double* __restrict__ ov, u32 n) {
-  u32 stride = gridDim.x * blockDim.x;
-  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    ok[i] = load_key<true>(src, i);
-    ov[i] = load_val<true>(src, i);
-  }
-}
-
 }  // namespace
 
-int choose_sort_bits(size_t n, int key_bits) {
-  (void)n;
-  if (key_bits <= 0) return 8;
-  // Fewest passes at 8..10 bit digits, preferring narrower digits on ties.
-  int best = 8, best_passes = (key_bits + 7) / 8;
-  for (int b = 9; b <= 10; ++b) {
-    int p = (key_bits + b - 1) / b;
+}  // namespace lnt
+
+#include "lnt_tuned.h"
+
+namespace lnt {
+
+int sort_variant_count() { return kNumVariants; }
+const SortVariant& sort_variant(int i) { return kVariants[i]; }
+
+int choose_sort_variant(size_t n, int key_bits) {
+  if (const char* e = getenv("LNT_SORT_VARIANT")) {
+    const int v = atoi(e);
+    if (v >= 0 && v < kNumVariants) return v;
+  }
+  // tuned table: first entry whose key-width and size ranges contain the request
+  for (const TunedSortEntry& t : kTunedSort) {
+    if (key_bits <= t.key_bits_max && n <= t.n_max && t.variant >= 0 && t.variant < kNumVariants)
+      return t.variant;
+  }
+  // untuned default: fewest passes, then the narrower digit
+  int best = 0, best_passes = 1 << 20;
+  for (int i = 0; i < kNumVariants; ++i) {
+    const int p = key_bits <= 0 ? 0 : (key_bits + kVariants[i].bits - 1) / kVariants[i].bits;
     if (p < best_passes) {
-      best = b;
+      best = i;
       best_passes = p;
     }
   }
   return best;
 }
 
-SortPlan make_sort_plan(size_t n, u64 max_key, int bits) {
+SortPlan make_sort_plan(size_t n, u64 max_key, int variant) {
   SortPlan p;
   p.key_bits = key_bits_for(max_key);
-  p.bits = bits;
-  p.passes = p.key_bits == 0 ? 0 : (p.key_bits + bits - 1) / bits;
+  p.variant = variant >= 0 && variant < kNumVariants ? variant : choose_sort_variant(n, p.key_bits);
+  const SortVariant& v = kVariants[p.variant];
+  p.bits = v.bits;
+  p.passes = p.key_bits == 0 ? 0 : (p.key_bits + v.bits - 1) / v.bits;
   p.n = (u32)n;
-  int items = bits <= 8 ? 16 : (bits <= 10 ? 12 : 8);
-  u32 tile = (u32)(kThreads * items);
-  p.ntiles = (u32)((n + tile - 1) / tile);
-  size_t radix = (size_t)1 << bits;
+  p.tile = (u32)(v.threads * v.items);
+  p.ntiles = (u32)((n + p.tile - 1) / p.tile);
+  const size_t radix = (size_t)1 << v.bits;
   size_t off = 0;
   p.off_ghist = off;
   off += align_up((size_t)std::max(p.passes, 1) * radix * 4, 256);
@@ -398,18 +522,20 @@ int run_sort(const SortPlan& plan, const PairSource& src, u64* buf0_k, double* b
              double* buf1_v, void* ctrl, cudaStream_t s) {
   if (plan.n == 0) return LNT_OK;
   if (plan.passes == 0) {
-    int blocks = std::max(1, std::min((int)((plan.n + 255) / 256), sm_count() * 8));
+    const int blocks = std::max(1, std::min((int)((plan.n + 255) / 256), sm_count() * 8));
     ProfScope prof("sort_copy", s);
     copy_source_kernel<<<blocks, 256, 0, s>>>(src, buf0_k, buf0_v, plan.n);
     count_launch();
     return launch_status();
   }
-  switch (plan.bits) {
-    case 8: return run_sort_bits<8>(plan, src, buf0_k, buf0_v, buf1_k, buf1_v, ctrl, s);
-    case 9: return run_sort_bits<9>(plan, src, buf0_k, buf0_v, buf1_k, buf1_v, ctrl, s);
-    case 10: return run_sort_bits<10>(plan, src, buf0_k, buf0_v, buf1_k, buf1_v, ctrl, s);
-    default: return LNT_UNSUPPORTED;
-  }
+  int i = 0;
+#define LNT_SV_CASE(B, T, I, W)                                                          \
+  if (plan.variant == i) return run_sort_variant<B, T, I, W>(plan, src, buf0_k, buf0_v, \
+                                                             buf1_k, buf1_v, ctrl, s);   \
+  ++i;
+  LNT_SORT_VARIANTS(LNT_SV_CASE)
+#undef LNT_SV_CASE
+  return LNT_UNSUPPORTED;
 }
 
 }  // namespace lnt
@@ -417,7 +543,7 @@ int run_sort(const SortPlan& plan, const PairSource& src, u64* buf0_k, double* b
 using namespace lnt;
 
 namespace {
-// Workspace of lnt_sort_pairs: [ctrl | tmp keys | tmp vals | (tmp2 keys | tmp2 vals)].
+// Workspace of lnt_sort_pairs: [ctrl | tmp keys | tmp vals | tmp2 keys | tmp2 vals].
 struct SortPairsLayout {
   SortPlan plan;
   size_t off_tk, off_tv, off_t2k, off_t2v, total;
@@ -425,8 +551,7 @@ struct SortPairsLayout {
 
 SortPairsLayout sort_pairs_layout(size_t n, u64 max_key) {
   SortPairsLayout L;
-  int kb = key_bits_for(max_key);
-  L.plan = make_sort_plan(n, max_key, choose_sort_bits(n, kb));
+  L.plan = make_sort_plan(n, max_key);
   size_t off = align_up(L.plan.ctrl_bytes, 256);
   L.off_tk = off;
   off += align_up(n * 8, 256);
@@ -442,6 +567,18 @@ SortPairsLayout sort_pairs_layout(size_t n, u64 max_key) {
 }  // namespace
 
 extern "C" {
+
+int lnt_sort_variant_count(void) { return sort_variant_count(); }
+
+int lnt_sort_variant(int index, int* bits, int* threads, int* items, int* window) {
+  if (index < 0 || index >= sort_variant_count() || !bits || !threads || !items || !window) return LNT_BAD_ARG;
+  const SortVariant& v = sort_variant(index);
+  *bits = v.bits;
+  *threads = v.threads;
+  *items = v.items;
+  *window = v.window;
+  return LNT_OK;
+}
 
 int lnt_sort_pairs_workspace(size_t n, uint64_t max_key, size_t* bytes) {
   if (!bytes) return LNT_BAD_ARG;
@@ -463,7 +600,8 @@ int lnt_sort_pairs(const uint64_t* keys_in, const double* vals_in, uint64_t* key
   u64* tk = reinterpret_cast<u64*>(ws + L.off_tk);
   double* tv = reinterpret_cast<double*>(ws + L.off_tv);
   PairSource src = plain_source((const u64*)keys_in, vals_in, n);
-  const bool inplace = (const void*)keys_in == (const void*)keys_out || (const void*)vals_in == (const void*)vals_out;
+  const bool inplace =
+      (const void*)keys_in == (const void*)keys_out || (const void*)vals_in == (const void*)vals_out;
   const int passes = L.plan.passes;
   if (!inplace || (passes % 2 == 0 && passes > 0)) {
     // pass 0 writes tmp when passes is even, so in-place is safe then.

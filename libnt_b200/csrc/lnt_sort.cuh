@@ -2,15 +2,20 @@
 //   1. hist_kernel: one read of all keys builds the digit histograms of every
 //      pass at once (shared-memory atomics, then one global add per bin);
 //      the last block to finish turns them into exclusive bin starts.
-//   2. per pass, onesweep_kernel: each CTA takes the next tile id, ranks its
-//      keys by digit with warp match-any + per-warp counters (stable), writes
-//      its per-digit counts to a look-back array, obtains its global offsets
-//      by decoupled look-back over predecessor tiles, reorders the tile in
-//      shared memory by digit and writes keys and values out in digit runs.
+//   2. per pass, onesweep_kernel: each CTA takes the next tile id, counts its
+//      tile's digits and publishes them at once, starts the value copy into
+//      shared memory (cp.async), obtains its global digit offsets by a
+//      windowed decoupled look-back over predecessor tiles, ranks its keys
+//      stably (warp ballots + per-warp counters), reorders keys and values in
+//      shared memory by digit and writes them out in digit runs.
 // Traffic per pass: 16 B read + 16 B written per pair (the HBM roofline).
 // The first pass reads through a PairSource, which concatenates two arrays
 // and re-keys each on the fly, so sortMerge's re-key + concatenation costs
 // no extra pass.
+//
+// Several kernel variants (digit width, CTA size, items per thread, look-back
+// window) are compiled in; the variant per (pair count, key width) comes from
+// the table written by the autotuner (libnt_b200/tune.py -> lnt_tuned.h).
 #pragma once
 
 #include "lnt_common.cuh"
@@ -46,27 +51,41 @@ inline PairSource plain_source(const u64* k, const double* v, size_t n) {
   return s;
 }
 
+// One compiled onesweep variant.
+struct SortVariant {
+  int bits;     // digit width
+  int threads;  // CTA size
+  int items;    // keys per thread (tile = threads * items)
+  int window;   // predecessors read per look-back round trip
+};
+
+int sort_variant_count();
+const SortVariant& sort_variant(int i);
+
 struct SortPlan {
+  int variant = 0;
   int key_bits = 0;
   int bits = 8;      // digit width
   int passes = 0;
   u32 n = 0;
+  u32 tile = 0;      // pairs per onesweep tile
   u32 ntiles = 0;    // onesweep tiles per pass
   // byte offsets inside the control block
   size_t off_ghist = 0, off_bstart = 0, off_status = 0, off_counters = 0, ctrl_bytes = 0;
 };
 
-// Fills a plan for n pairs with keys < max_key and digit width `bits`.
-SortPlan make_sort_plan(size_t n, u64 max_key, int bits);
+// Variant for a sort of n pairs with key_bits significant bits: the
+// environment variable LNT_SORT_VARIANT when set (used by the autotuner),
+// else the tuned table.
+int choose_sort_variant(size_t n, int key_bits);
+
+// Fills a plan for n pairs with keys < max_key (variant < 0: choose).
+SortPlan make_sort_plan(size_t n, u64 max_key, int variant = -1);
 
 // Runs the passes.  Pass p reads the previous pass's output (pass 0 reads
 // src) and writes buffer ((passes-1-p) & 1): buf0 = final destination.
 // `ctrl` points at plan.ctrl_bytes of scratch, zeroed here.
 int run_sort(const SortPlan& plan, const PairSource& src, u64* buf0_k, double* buf0_v, u64* buf1_k,
              double* buf1_v, void* ctrl, cudaStream_t s);
-
-// Digit width chosen for a sort of n pairs with key_bits significant bits
-// (table written by the autotuner; defaults when absent).
-int choose_sort_bits(size_t n, int key_bits);
 
 }  // namespace lnt

@@ -68,6 +68,24 @@ def test_sort_pairs_bit_exact(cuda, torch, rng, n, bits):
     assert cuda.device_status() == 0
 
 
+@pytest.mark.parametrize("variant", range(12))
+@pytest.mark.parametrize("n,bits", [(1, 9), (3071, 36), (12289, 20), (300007, 36), (200000, 63), (65537, 10)])
+def test_every_sort_variant_bit_exact(cuda, torch, rng, monkeypatch, variant, n, bits):
+    """Each compiled kernel variant (the autotuner may pick any) is stable and exact."""
+    import libnt_b200 as L
+    if variant >= L.lib().lnt_sort_variant_count():
+        pytest.skip("variant not compiled")
+    monkeypatch.setenv("LNT_SORT_VARIANT", str(variant))
+    keys = rng.integers(0, 2 ** bits, n, dtype=np.uint64)
+    keys[: n // 3] = keys[n // 2]
+    vals = rng.standard_normal(n)
+    k, v = cuda.sort_pairs(to_dev(keys, torch), to_dev(vals, torch), max_key=2 ** bits)
+    ek, ev = oracle.sort_pairs(keys, vals)
+    np.testing.assert_array_equal(to_host(k, np.uint64), ek)
+    np.testing.assert_array_equal(to_host(v), ev)
+    assert cuda.device_status() == 0
+
+
 def test_sort_pairs_in_place_and_duplicates(cuda, torch, rng):
     n = 300001
     keys = rng.integers(0, 1000, n, dtype=np.uint64)  # heavy duplicates
