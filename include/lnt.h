@@ -154,6 +154,35 @@ LNT_API int lnt_sort_reduce(const uint64_t* a_keys, const double* a_vals, size_t
                     uint64_t* keys_out, double* vals_out, uint64_t* d_nout,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- scan merge (operands sorted in the same linearisation) ------------- */
+
+LNT_API int lnt_merge_sorted_workspace(size_t na, size_t nb, size_t* bytes);
+
+/* Merge two key-sorted operands: A-only entries are copied, B-only entries
+ * become op(0, b), equal keys op(a, b) (op 0 = +, 1 = -); within a run of
+ * equal keys the j-th A pairs with the j-th B.  Every entry is kept, exact
+ * zeros included.  Replaces outside_merge_sparse_storage_containers
+ * (FunctionUtil.h:373-419) on the SparseMIABase::outside_scanMerge path
+ * (SparseMIABase.h:1404-1455) and the mex gateway SparseMergeMex
+ * (MATLAB/mex/sparse_merge.cpp:15-163).  c arrays need room for na + nb
+ * pairs; *d_nout (device) receives the output count. */
+LNT_API int lnt_merge_sorted(const uint64_t* a_keys, const double* a_vals, size_t na,
+                             const uint64_t* b_keys, const double* b_vals, size_t nb, int op,
+                             uint64_t* c_keys, double* c_vals, uint64_t* d_nout,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- re-key + sort (sort under a new linearisation) --------------------- */
+
+LNT_API int lnt_permute_sort_workspace(size_t n, uint64_t max_key, size_t* bytes);
+
+/* Re-key (may be NULL: keys as they are) and stable-sort n pairs, out of
+ * place.  Replaces SparseMIABase::sort(seq) (SparseMIABase.h:590-645: re-key,
+ * then radix sort or RadixShuffle::permute, LibMIARadix.h:705-927) and the mex
+ * gateway SparsePermuteMex (MATLAB/mex/sparse_permute.cpp:15-117). */
+LNT_API int lnt_permute_sort(const uint64_t* keys_in, const double* vals_in, size_t n,
+                             const lnt_rekey_spec* rekey, uint64_t* keys_out, double* vals_out,
+                             uint64_t max_key, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,10 @@ _SIGS = {
     "lnt_sort_reduce_workspace": ([_sz, _sz, C.c_uint64, C.POINTER(C.c_size_t)], C.c_int),
     "lnt_sort_reduce": ([_vp, _vp, _sz, C.POINTER(RekeySpec), _vp, _vp, _sz, C.POINTER(RekeySpec), C.c_double,
                          C.c_uint64, C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
+    "lnt_merge_sorted_workspace": ([_sz, _sz, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_merge_sorted": ([_vp, _vp, _sz, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
+    "lnt_permute_sort_workspace": ([_sz, C.c_uint64, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_permute_sort": ([_vp, _vp, _sz, C.POINTER(RekeySpec), _vp, _vp, C.c_uint64, _vp, _sz, _vp], C.c_int),
 }
 
 _lib = None
@@ -244,3 +248,47 @@ def sort_reduce(a_keys, a_vals, b_keys=None, b_vals=None, *, max_key: int, a_rek
         return ok, ov, cnt
     m = int(cnt.item())
     return ok[:m], ov[:m]
+
+
+def merge_sorted(a_keys, a_vals, b_keys, b_vals, op: int = 0, out_keys=None, out_vals=None, count=None,
+                 ws=None, sync: bool = True):
+    """Scan merge of two key-sorted operands (op 0 = +, 1 = -)."""
+    torch = _torch()
+    na, nb = a_keys.numel(), b_keys.numel()
+    dev = a_keys.device
+    ok = torch.empty(na + nb, dtype=torch.int64, device=dev) if out_keys is None else out_keys
+    ov = torch.empty(na + nb, dtype=torch.float64, device=dev) if out_vals is None else out_vals
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev) if count is None else count
+    b = C.c_size_t(0)
+    _check(lib().lnt_merge_sorted_workspace(na, nb, C.byref(b)), "lnt_merge_sorted_workspace")
+    if ws is None or ws.numel() < b.value:
+        ws = workspace(b.value, dev)
+    st = lib().lnt_merge_sorted(_ptr(a_keys), _ptr(a_vals), na, _ptr(b_keys), _ptr(b_vals), nb, int(op), _ptr(ok),
+                                _ptr(ov), _ptr(cnt), _ptr(ws), ws.numel(), _stream())
+    _check(st, "lnt_merge_sorted")
+    if not sync:
+        return ok, ov, cnt
+    m = int(cnt.item())
+    return ok[:m], ov[:m]
+
+
+def permute_sort_workspace(n: int, max_key: int) -> int:
+    b = C.c_size_t(0)
+    _check(lib().lnt_permute_sort_workspace(n, int(max_key), C.byref(b)), "lnt_permute_sort_workspace")
+    return b.value
+
+
+def permute_sort(keys, vals, *, max_key: int, rekey: RekeySpec | None = None, out_keys=None, out_vals=None,
+                 ws=None):
+    """Re-key (optional) and stable sort, out of place."""
+    torch = _torch()
+    n = keys.numel()
+    ok = torch.empty_like(keys) if out_keys is None else out_keys
+    ov = torch.empty_like(vals) if out_vals is None else out_vals
+    need = permute_sort_workspace(n, max_key)
+    if ws is None or ws.numel() < need:
+        ws = workspace(need, keys.device)
+    st = lib().lnt_permute_sort(_ptr(keys), _ptr(vals), n, C.byref(rekey) if rekey else None, _ptr(ok), _ptr(ov),
+                                int(max_key), _ptr(ws), ws.numel(), _stream())
+    _check(st, "lnt_permute_sort")
+    return ok, ov
