@@ -183,6 +183,39 @@ LNT_API int lnt_permute_sort(const uint64_t* keys_in, const double* vals_in, siz
                              const lnt_rekey_spec* rekey, uint64_t* keys_out, double* vals_out,
                              uint64_t max_key, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- sparse lattice product -------------------------------------------- */
+
+/* A sparse lattice (3-D sparse array: rows x cols x tabs) in column-major LCO
+ * form: key = row + rows*(col + cols*tab), keys ascending
+ * (SparseLatticeBase / MappedSparseLattice, MappedSparseLattice.h:163-263). */
+typedef struct lnt_lattice {
+    const uint64_t* keys;
+    const double* vals;
+    uint64_t nnz;
+    int64_t rows, cols, tabs;
+} lnt_lattice;
+
+/* C(:,:,t) = A(:,:,t) * B(:,:,t) for every tab; C is rows(A) x cols(B) x tabs,
+ * keys ascending, duplicate products summed, exact zeros kept.  Replaces
+ * SparseLatticeBase::operator* -> csc_no_accum<true> (SparseLatticeBase.h:
+ * 1572-1576, 1854-1990) and the mex gateway SparseLatticeMultMex with alg 0
+ * (MATLAB/mex/sparselattice_mul.cpp:14-137).  Two phases:
+ *   1. lnt_lattice_mult_plan fills `plan` (size from *_plan_workspace) and
+ *      writes d_counts[0] = number of products, d_counts[1] = capacity C needs
+ *      (the exact output count, or an upper bound);
+ *   2. lnt_lattice_mult (workspace from lnt_lattice_mult_workspace with the
+ *      product count) writes C and *d_nc.
+ * Errors: LNT_BAD_DIMS when cols(A) != rows(B) or the tab counts differ
+ * (SparseLatticeBase::check_mult_dims). */
+LNT_API int lnt_lattice_mult_plan_workspace(const lnt_lattice* A, const lnt_lattice* B, size_t* bytes);
+LNT_API int lnt_lattice_mult_plan(const lnt_lattice* A, const lnt_lattice* B, void* plan,
+                                  size_t plan_bytes, uint64_t* d_counts, void* stream);
+LNT_API int lnt_lattice_mult_workspace(const lnt_lattice* A, const lnt_lattice* B, uint64_t products,
+                                       size_t* bytes);
+LNT_API int lnt_lattice_mult(const lnt_lattice* A, const lnt_lattice* B, const void* plan,
+                             uint64_t products, void* workspace, size_t workspace_bytes,
+                             uint64_t* c_keys, double* c_vals, uint64_t* d_nc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,17 @@ class LntError(RuntimeError):
         super().__init__(f"{what}: lnt status {status} ({STATUS.get(status, 'unknown')})")
 
 
+class Lattice(C.Structure):
+    """lnt_lattice (include/lnt.h)."""
+    _fields_ = [("keys", C.c_void_p), ("vals", C.c_void_p), ("nnz", C.c_uint64), ("rows", C.c_int64),
+                ("cols", C.c_int64), ("tabs", C.c_int64)]
+
+    @classmethod
+    def of(cls, keys, vals, rows, cols, tabs=1) -> "Lattice":
+        return cls(keys.data_ptr() if keys.numel() else None, vals.data_ptr() if vals.numel() else None,
+                   keys.numel(), rows, cols, tabs)
+
+
 class RekeySpec(C.Structure):
     """lnt_rekey_spec (include/lnt.h)."""
     _fields_ = [("order", C.c_int32), ("cur_seq", C.c_int32 * MAX_ORDER), ("new_seq", C.c_int32 * MAX_ORDER),
@@ -71,6 +82,12 @@ _SIGS = {
     "lnt_merge_sorted": ([_vp, _vp, _sz, _vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
     "lnt_permute_sort_workspace": ([_sz, C.c_uint64, C.POINTER(C.c_size_t)], C.c_int),
     "lnt_permute_sort": ([_vp, _vp, _sz, C.POINTER(RekeySpec), _vp, _vp, C.c_uint64, _vp, _sz, _vp], C.c_int),
+    "lnt_lattice_mult_plan_workspace": ([C.POINTER(Lattice), C.POINTER(Lattice), C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_lattice_mult_plan": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, _sz, _vp, _vp], C.c_int),
+    "lnt_lattice_mult_workspace": ([C.POINTER(Lattice), C.POINTER(Lattice), C.c_uint64, C.POINTER(C.c_size_t)],
+                                   C.c_int),
+    "lnt_lattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, C.c_uint64, _vp, _sz, _vp, _vp, _vp, _vp],
+                         C.c_int),
 }
 
 _lib = None
@@ -292,3 +309,29 @@ def permute_sort(keys, vals, *, max_key: int, rekey: RekeySpec | None = None, ou
                                 int(max_key), _ptr(ws), ws.numel(), _stream())
     _check(st, "lnt_permute_sort")
     return ok, ov
+
+
+def lattice_mult(a_keys, a_vals, b_keys, b_vals, h: int, w: int, wB: int, d: int = 1):
+    """Sparse lattice product (column-major keys, both key-sorted); returns
+    trimmed (keys, vals) of C (h x wB x d) and the product count."""
+    torch = _torch()
+    A = Lattice.of(a_keys, a_vals, h, w, d)
+    B = Lattice.of(b_keys, b_vals, w, wB, d)
+    dev = a_keys.device
+    b = C.c_size_t(0)
+    _check(lib().lnt_lattice_mult_plan_workspace(C.byref(A), C.byref(B), C.byref(b)), "lnt_lattice_mult_plan_workspace")
+    plan = workspace(b.value, dev)
+    counts = torch.zeros(2, dtype=torch.int64, device=dev)
+    _check(lib().lnt_lattice_mult_plan(C.byref(A), C.byref(B), _ptr(plan), plan.numel(), _ptr(counts), _stream()),
+           "lnt_lattice_mult_plan")
+    products, cap = (int(x) for x in counts.tolist())
+    _check(lib().lnt_lattice_mult_workspace(C.byref(A), C.byref(B), products, C.byref(b)),
+           "lnt_lattice_mult_workspace")
+    ws = workspace(b.value, dev)
+    ck = torch.empty(max(cap, 1), dtype=torch.int64, device=dev)
+    cv = torch.empty(max(cap, 1), dtype=torch.float64, device=dev)
+    nc = torch.zeros(1, dtype=torch.int64, device=dev)
+    _check(lib().lnt_lattice_mult(C.byref(A), C.byref(B), _ptr(plan), products, _ptr(ws), ws.numel(), _ptr(ck),
+                                  _ptr(cv), _ptr(nc), _stream()), "lnt_lattice_mult")
+    m = int(nc.item())
+    return ck[:m], cv[:m], products
