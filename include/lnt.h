@@ -216,6 +216,32 @@ LNT_API int lnt_lattice_mult(const lnt_lattice* A, const lnt_lattice* B, const v
                              uint64_t products, void* workspace, size_t workspace_bytes,
                              uint64_t* c_keys, double* c_vals, uint64_t* d_nc, void* stream);
 
+/* ---- batched lattice products ------------------------------------------- */
+
+/* `count` independent products C_p = A_p * B_p, each as lnt_lattice_mult,
+ * with at most 1024 rows per A_p.  Host arrays: dims_host[4p..4p+3] =
+ * (rows(A_p), cols(A_p) = rows(B_p), cols(B_p), tabs); a_off_host / b_off_host
+ * (count+1 entries) delimit each problem's operand inside the concatenated
+ * device arrays a_keys/a_vals, b_keys/b_vals (each lattice key-sorted).
+ * C_p is written at c_keys/c_vals + c_off[p] (device, count+1 entries);
+ * *c_capacity bounds the total output.  The reference has no batched form:
+ * it is a loop of csc_no_accum calls (SparseLatticeBase.h:1854-1990).
+ * Call lnt_batched_prepare once per batch layout (it uploads the descriptor
+ * tables into the workspace, synchronously), then lnt_batched_lattice_mult,
+ * which only enqueues kernels and memsets on `stream` and can therefore be
+ * captured into a CUDA graph and replayed.  Chunk size of the work queue:
+ * LNT_BATCH_CHUNK from the environment (default 8). */
+LNT_API int lnt_batched_workspace(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                                  const uint64_t* b_off_host, size_t* bytes, uint64_t* c_capacity);
+LNT_API int lnt_batched_prepare(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                                const uint64_t* b_off_host, void* workspace, size_t workspace_bytes,
+                                void* stream);
+LNT_API int lnt_batched_lattice_mult(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                                     const uint64_t* b_off_host, const uint64_t* a_keys,
+                                     const double* a_vals, const uint64_t* b_keys, const double* b_vals,
+                                     void* workspace, size_t workspace_bytes, uint64_t* c_keys,
+                                     double* c_vals, uint64_t* d_c_off, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

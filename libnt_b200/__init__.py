@@ -88,6 +88,9 @@ _SIGS = {
                                    C.c_int),
     "lnt_lattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, C.c_uint64, _vp, _sz, _vp, _vp, _vp, _vp],
                          C.c_int),
+    "lnt_batched_workspace": ([C.c_int, _vp, _vp, _vp, C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)], C.c_int),
+    "lnt_batched_prepare": ([C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
+    "lnt_batched_lattice_mult": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp], C.c_int),
 }
 
 _lib = None
@@ -335,3 +338,43 @@ def lattice_mult(a_keys, a_vals, b_keys, b_vals, h: int, w: int, wB: int, d: int
                                   _ptr(cv), _ptr(nc), _stream()), "lnt_lattice_mult")
     m = int(nc.item())
     return ck[:m], cv[:m], products
+
+
+class Batch:
+    """A batch of lattice products on one device (see lnt_batched_* in include/lnt.h).
+
+    dims: int64 array (count, 4) of (h, w, wB, d); a_off / b_off: uint64 (count+1)
+    offsets into the concatenated device tensors a_keys/a_vals, b_keys/b_vals."""
+
+    def __init__(self, dims, a_off, b_off, a_keys, a_vals, b_keys, b_vals):
+        torch = _torch()
+        self.count = int(len(dims))
+        self.dims = np.ascontiguousarray(dims, np.int64)
+        self.a_off = np.ascontiguousarray(a_off, np.uint64)
+        self.b_off = np.ascontiguousarray(b_off, np.uint64)
+        self.tensors = (a_keys, a_vals, b_keys, b_vals)
+        dev = a_keys.device
+        nb = C.c_size_t(0)
+        cap = C.c_uint64(0)
+        _check(lib().lnt_batched_workspace(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
+                                           self.b_off.ctypes.data, C.byref(nb), C.byref(cap)), "lnt_batched_workspace")
+        self.ws = workspace(nb.value, dev)
+        self.capacity = int(cap.value)
+        self.c_keys = torch.empty(max(self.capacity, 1), dtype=torch.int64, device=dev)
+        self.c_vals = torch.empty(max(self.capacity, 1), dtype=torch.float64, device=dev)
+        self.c_off = torch.zeros(self.count + 1, dtype=torch.int64, device=dev)
+        _check(lib().lnt_batched_prepare(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
+                                         self.b_off.ctypes.data, _ptr(self.ws), self.ws.numel(), _stream()),
+               "lnt_batched_prepare")
+
+    def run(self):
+        """Enqueue the batched product on the current stream (capturable)."""
+        ak, av, bk, bv = self.tensors
+        _check(lib().lnt_batched_lattice_mult(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
+                                              self.b_off.ctypes.data, _ptr(ak), _ptr(av), _ptr(bk), _ptr(bv),
+                                              _ptr(self.ws), self.ws.numel(), _ptr(self.c_keys), _ptr(self.c_vals),
+                                              _ptr(self.c_off), _stream()), "lnt_batched_lattice_mult")
+
+    def result(self, p):
+        off = self.c_off.tolist()
+        return self.c_keys[off[p]:off[p + 1]], self.c_vals[off[p]:off[p + 1]]

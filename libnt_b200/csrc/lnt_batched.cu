@@ -1,0 +1,351 @@
+// Batched sparse lattice products: thousands of independent, unevenly sized
+// C_p = A_p * B_p (each as in lnt_lattice_mult) in a fixed number of launches,
+// all stream-ordered and capturable in one CUDA graph.  The reference has no
+// batching: its equivalent is a loop of csc_no_accum calls
+// (SparseLatticeBase.h:1854-1990), one per contraction.
+//
+// Layout: operands are concatenated (A of problem p at a_off[p] .. a_off[p+1],
+// likewise B); a descriptor per problem holds its dims, magic dividers and
+// offsets into the scratch tables.  Output C is concatenated too; problem p's
+// part starts at c_off[p].
+//
+// Pipeline (per call):
+//   colptr (A and B): dense column pointers of every problem (u32 offsets);
+//   spa<symbolic>: persistent warps pull chunks of output columns ("units") of
+//     all problems from an atomic queue and count each column's output rows;
+//   scan: global exclusive sum over units -> output position of every column;
+//   spa<numeric>: persistent warps pull chunks again and write each column's
+//     rows (dense accumulator in shared memory, ascending emission);
+//   coff: per-problem output offsets.
+// The queue chunk size (units per grab) is the segment-split knob the
+// autotuner sets: small chunks balance uneven columns, large ones cut queue
+// traffic.
+#include <algorithm>
+#include <cstdlib>
+#include <vector>
+
+#include "lnt_scan.cuh"
+
+namespace lnt {
+namespace {
+
+constexpr int kMaxRows = 1024;  // accumulator rows per warp
+constexpr int kWarps = 4;
+
+struct ProbDesc {
+  u64 a_off, a_n, b_off, b_n;
+  u64 aptr_off, bptr_off;  // into the u32 pointer tables
+  u64 unit_off, units;     // global unit range (units = wB * d)
+  u64 h, w, wB, d;
+  Divider div_h, div_w, div_wB;
+};
+
+struct BatchArgs {
+  const u64* ak;
+  const double* av;
+  const u64* bk;
+  const double* bv;
+  const ProbDesc* prob;
+  int count;
+  u64 total_units;
+  u32* aptr;
+  u32* bptr;
+};
+
+__device__ __forceinline__ int find_problem_by_unit(const ProbDesc* prob, int count, u64 u) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prob[mid].unit_off <= u) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Column pointers of every problem's A (which == 0) or B (which == 1).
+// Position q enumerates, problem by problem, the n_p + 1 boundaries.
+__global__ void batch_colptr_kernel(BatchArgs args, int which, const u64* __restrict__ pos_off, u64 total_pos) {
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 q = (u64)blockIdx.x * blockDim.x + threadIdx.x; q < total_pos; q += stride) {
+    int lo = 0, hi = args.count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pos_off[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    const ProbDesc& P = args.prob[lo];
+    const u64 i = q - pos_off[lo];
+    const u64 n = which == 0 ? P.a_n : P.b_n;
+    const u64* keys = which == 0 ? args.ak + P.a_off : args.bk + P.b_off;
+    const Divider& dv = which == 0 ? P.div_h : P.div_w;
+    const u64 ncol = which == 0 ? P.w * P.d : P.units;
+    u32* ptr = (which == 0 ? args.aptr + P.aptr_off : args.bptr + P.bptr_off);
+    const long long prev = i == 0 ? -1ll : (long long)min(divide(keys[i - 1], dv), ncol);
+    const u64 cur = i == n ? ncol : min(divide(keys[i], dv), ncol);
+    for (long long c = prev + 1; c <= (long long)cur; ++c) ptr[c] = (u32)i;
+  }
+}
+
+template <bool NUMERIC>
+__global__ void __launch_bounds__(kWarps * 32) batch_spa_kernel(BatchArgs args, u32 chunk, u32* __restrict__ queue,
+                                                                 u64* __restrict__ ucount,
+                                                                 const u64* __restrict__ uoff,
+                                                                 u64* __restrict__ ck, double* __restrict__ cv) {
+  __shared__ u32 s_bits[kWarps][kMaxRows / 32];
+  __shared__ double s_acc[NUMERIC ? kWarps : 1][NUMERIC ? kMaxRows : 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u32* bits = s_bits[warp];
+  double* acc = s_acc[NUMERIC ? warp : 0];
+  while (true) {
+    u64 first = 0;
+    if (lane == 0) first = (u64)atomicAdd(queue, chunk);
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (first >= args.total_units) break;
+    const u64 last = min(first + chunk, args.total_units);
+    int p = find_problem_by_unit(args.prob, args.count, first);
+    for (u64 u = first; u < last; ++u) {
+      while (u >= args.prob[p].unit_off + args.prob[p].units) ++p;  // chunks may span problems
+      const ProbDesc& P = args.prob[p];
+      const u64 lu = u - P.unit_off;  // column id within the problem: col + wB*tab
+      const u32* bptr = args.bptr + P.bptr_off;
+      const u64 e0 = bptr[lu], e1 = bptr[lu + 1];
+      if (e0 == e1) {
+        if (!NUMERIC && lane == 0) ucount[u] = 0;
+        continue;
+      }
+      const u64 h = P.h, w = P.w;
+      const int hw = (int)((h + 31) / 32);
+      for (int i = lane; i < hw; i += 32) bits[i] = 0u;
+      if (NUMERIC)
+        for (int i = lane; i < (int)h; i += 32) acc[i] = 0.0;
+      __syncwarp();
+      const u64 t = divide(lu, P.div_wB);
+      const u64* ak = args.ak + P.a_off;
+      const double* av = args.av + P.a_off;
+      const u64* bk = args.bk + P.b_off;
+      const double* bv = args.bv + P.b_off;
+      const u32* aptr = args.aptr + P.aptr_off;
+      for (u64 e = e0 + lane; e < e1; e += 32) {
+        const u64 acol = (bk[e] - w * lu) + w * t;
+        const u32 lo = aptr[acol], hi = aptr[acol + 1];
+        const double beta = NUMERIC ? bv[e] : 0.0;
+        for (u32 x = lo; x < hi; ++x) {
+          const u32 r = (u32)(ak[x] - acol * h);
+          atomicOr(&bits[r >> 5], 1u << (r & 31));
+          if (NUMERIC) atomicAdd(&acc[r], av[x] * beta);
+        }
+      }
+      __syncwarp();
+      if (!NUMERIC) {
+        u32 c = 0;
+        for (int i = lane; i < hw; i += 32) c += __popc(bits[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) ucount[u] = c;
+      } else {
+        u64 out = uoff[u];
+        const u64 colkey = h * lu;
+        for (int g = 0; g < hw; ++g) {
+          const u32 word = bits[g];
+          if (word & (1u << lane)) {
+            const u32 r = (u32)g * 32 + lane;
+            const u64 o = out + __popc(word & ((1u << lane) - 1u));
+            ck[o] = colkey + r;
+            cv[o] = acc[r];
+          }
+          out += __popc(word);
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void batch_coff_kernel(const ProbDesc* __restrict__ prob, int count, const u64* __restrict__ uoff,
+                                  u64 total_units, u64* __restrict__ c_off) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < count) c_off[p] = uoff[prob[p].unit_off];
+  if (p == count) c_off[count] = uoff[total_units];
+}
+
+struct BatchLayout {
+  u64 total_units, aptr_len, bptr_len, a_pos, b_pos, c_bound;
+  size_t off_prob, off_apos, off_bpos, off_aptr, off_bptr, off_ucount, off_uoff, off_queue, off_scan, total;
+};
+
+int batch_layout(int count, const int64_t* dims, const uint64_t* a_off, const uint64_t* b_off, BatchLayout* L,
+                 std::vector<ProbDesc>* descs, std::vector<u64>* apos, std::vector<u64>* bpos) {
+  if (count <= 0 || !dims || !a_off || !b_off) return LNT_BAD_ARG;
+  L->total_units = L->aptr_len = L->bptr_len = L->a_pos = L->b_pos = L->c_bound = 0;
+  if (descs) descs->resize(count);
+  if (apos) apos->resize(count);
+  if (bpos) bpos->resize(count);
+  for (int p = 0; p < count; ++p) {
+    const int64_t h = dims[4 * p], w = dims[4 * p + 1], wB = dims[4 * p + 2], d = dims[4 * p + 3];
+    if (h <= 0 || w <= 0 || wB <= 0 || d <= 0) return LNT_BAD_DIMS;
+    if (h > kMaxRows) return LNT_UNSUPPORTED;
+    if (a_off[p + 1] < a_off[p] || b_off[p + 1] < b_off[p]) return LNT_BAD_ARG;
+    const u64 na = a_off[p + 1] - a_off[p], nb = b_off[p + 1] - b_off[p];
+    if (na >= (1ull << 32) || nb >= (1ull << 32)) return LNT_UNSUPPORTED;
+    unsigned __int128 ka = (unsigned __int128)h * w * d, kb = (unsigned __int128)w * wB * d;
+    if ((ka >> 63) || (kb >> 63)) return LNT_OVERFLOW_KEYBITS;
+    if (descs) {
+      ProbDesc& P = (*descs)[p];
+      P.a_off = a_off[p];
+      P.a_n = na;
+      P.b_off = b_off[p];
+      P.b_n = nb;
+      P.aptr_off = L->aptr_len;
+      P.bptr_off = L->bptr_len;
+      P.unit_off = L->total_units;
+      P.units = (u64)wB * d;
+      P.h = h;
+      P.w = w;
+      P.wB = wB;
+      P.d = d;
+      P.div_h = make_divider(h);
+      P.div_w = make_divider(w);
+      P.div_wB = make_divider(wB);
+    }
+    if (apos) (*apos)[p] = L->a_pos;
+    if (bpos) (*bpos)[p] = L->b_pos;
+    L->aptr_len += (u64)w * d + 1;
+    L->bptr_len += (u64)wB * d + 1;
+    L->total_units += (u64)wB * d;
+    L->a_pos += na + 1;
+    L->b_pos += nb + 1;
+    L->c_bound += (u64)std::min<unsigned __int128>((unsigned __int128)h * wB * d, (unsigned __int128)nb * h);
+  }
+  size_t off = 0;
+  L->off_prob = off;
+  off += align_up((size_t)count * sizeof(ProbDesc), 256);
+  L->off_apos = off;
+  off += align_up((size_t)count * 8, 256);
+  L->off_bpos = off;
+  off += align_up((size_t)count * 8, 256);
+  L->off_aptr = off;
+  off += align_up(L->aptr_len * 4, 256);
+  L->off_bptr = off;
+  off += align_up(L->bptr_len * 4, 256);
+  L->off_ucount = off;
+  off += align_up((L->total_units + 1) * 8, 256);
+  L->off_uoff = off;
+  off += align_up((L->total_units + 1) * 8, 256);
+  L->off_queue = off;
+  off += 256;
+  L->off_scan = off;
+  off += align_up(scan::workspace_bytes(L->total_units), 256);
+  L->total = off;
+  return LNT_OK;
+}
+
+struct U64Of {
+  const u64* v;
+  __device__ __forceinline__ u64 operator()(size_t i) const { return v[i]; }
+};
+
+u32 batch_chunk() {
+  if (const char* e = getenv("LNT_BATCH_CHUNK")) {
+    const int c = atoi(e);
+    if (c >= 1 && c <= 4096) return (u32)c;
+  }
+  return 8;
+}
+
+}  // namespace
+}  // namespace lnt
+
+using namespace lnt;
+
+extern "C" {
+
+int lnt_batched_workspace(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                          const uint64_t* b_off_host, size_t* bytes, uint64_t* c_capacity) {
+  if (!bytes) return LNT_BAD_ARG;
+  BatchLayout L;
+  int st = batch_layout(count, dims_host, a_off_host, b_off_host, &L, nullptr, nullptr, nullptr);
+  if (st != LNT_OK) return st;
+  *bytes = L.total;
+  if (c_capacity) *c_capacity = L.c_bound;
+  return LNT_OK;
+}
+
+int lnt_batched_prepare(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                        const uint64_t* b_off_host, void* workspace, size_t workspace_bytes, void* stream) {
+  BatchLayout L;
+  std::vector<ProbDesc> descs;
+  std::vector<u64> apos, bpos;
+  int st = batch_layout(count, dims_host, a_off_host, b_off_host, &L, &descs, &apos, &bpos);
+  if (st != LNT_OK) return st;
+  if (!workspace || workspace_bytes < L.total || (uintptr_t)workspace % 256) return LNT_WORKSPACE;
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  cudaStream_t s = as_stream(stream);
+  // synchronous copies: the host vectors die with this call
+  if (cudaStreamSynchronize(s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  if (cudaMemcpy(w + L.off_prob, descs.data(), descs.size() * sizeof(ProbDesc), cudaMemcpyHostToDevice) != cudaSuccess)
+    return LNT_DEVICE_ERROR;
+  if (cudaMemcpy(w + L.off_apos, apos.data(), apos.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    return LNT_DEVICE_ERROR;
+  if (cudaMemcpy(w + L.off_bpos, bpos.data(), bpos.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    return LNT_DEVICE_ERROR;
+  return LNT_OK;
+}
+
+int lnt_batched_lattice_mult(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                             const uint64_t* b_off_host, const uint64_t* a_keys, const double* a_vals,
+                             const uint64_t* b_keys, const double* b_vals, void* workspace, size_t workspace_bytes,
+                             uint64_t* c_keys, double* c_vals, uint64_t* d_c_off, void* stream) {
+  BatchLayout L;
+  int st = batch_layout(count, dims_host, a_off_host, b_off_host, &L, nullptr, nullptr, nullptr);
+  if (st != LNT_OK) return st;
+  if (!workspace || workspace_bytes < L.total || (uintptr_t)workspace % 256) return LNT_WORKSPACE;
+  if (!d_c_off) return LNT_BAD_ARG;
+  if ((L.a_pos > (u64)count && (!a_keys || !a_vals)) || (L.b_pos > (u64)count && (!b_keys || !b_vals)))
+    return LNT_BAD_ARG;
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  cudaStream_t s = as_stream(stream);
+  BatchArgs args;
+  args.ak = (const u64*)a_keys;
+  args.av = a_vals;
+  args.bk = (const u64*)b_keys;
+  args.bv = b_vals;
+  args.prob = reinterpret_cast<const ProbDesc*>(w + L.off_prob);
+  args.count = count;
+  args.total_units = L.total_units;
+  args.aptr = reinterpret_cast<u32*>(w + L.off_aptr);
+  args.bptr = reinterpret_cast<u32*>(w + L.off_bptr);
+  u64* ucount = reinterpret_cast<u64*>(w + L.off_ucount);
+  u64* uoff = reinterpret_cast<u64*>(w + L.off_uoff);
+  u32* queue = reinterpret_cast<u32*>(w + L.off_queue);
+  const int sms = sm_count();
+  if (cudaMemsetAsync(queue, 0, 256, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  {
+    ProfScope prof("batch_colptr", s);
+    const int ga = (int)std::max<u64>(1, std::min<u64>((L.a_pos + 255) / 256, (u64)sms * 16));
+    batch_colptr_kernel<<<ga, 256, 0, s>>>(args, 0, reinterpret_cast<const u64*>(w + L.off_apos), L.a_pos);
+    const int gb = (int)std::max<u64>(1, std::min<u64>((L.b_pos + 255) / 256, (u64)sms * 16));
+    batch_colptr_kernel<<<gb, 256, 0, s>>>(args, 1, reinterpret_cast<const u64*>(w + L.off_bpos), L.b_pos);
+    count_launch(2);
+  }
+  const u32 chunk = batch_chunk();
+  {
+    ProfScope prof("batch_spa_symbolic", s);
+    batch_spa_kernel<false><<<sms * 8, kWarps * 32, 0, s>>>(args, chunk, queue, ucount, nullptr, nullptr, nullptr);
+    count_launch();
+  }
+  st = scan::run(U64Of{ucount}, L.total_units, (unsigned long long*)uoff, nullptr, w + L.off_scan, s, "batch_scan");
+  if (st != LNT_OK) return st;
+  {
+    ProfScope prof("batch_spa_numeric", s);
+    batch_spa_kernel<true><<<sms * 6, kWarps * 32, 0, s>>>(args, chunk, queue + 1, nullptr, uoff, (u64*)c_keys,
+                                                           c_vals);
+    count_launch();
+  }
+  {
+    ProfScope prof("batch_coff", s);
+    batch_coff_kernel<<<(count + 1 + 255) / 256, 256, 0, s>>>(args.prob, count, uoff, L.total_units,
+                                                               (u64*)d_c_off);
+    count_launch();
+  }
+  return launch_status();
+}
+
+}  // extern "C"
