@@ -363,6 +363,329 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# other workloads (--workload ...): one JSON line each, same contract keys
+# ---------------------------------------------------------------------------
+def _line(metric_unit, value, ms, args, world, config, extra):
+    d = {"metric": METRIC, "value": value, "unit": metric_unit, "n_gpus": world, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config}
+    d.update(extra)
+    return d
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def contraction_inputs(seed=0):
+    """c(i,l) = a(i,j,k) * b(k,l,j): order-3 SparseMIA, dims 100^3, 10^4 distinct
+    coordinates each (uniform without replacement), values U[-1,1], seed 0."""
+    rng = np.random.default_rng(seed)
+    ak = rng.choice(10 ** 6, 10 ** 4, replace=False).astype(np.uint64)
+    bk = rng.choice(10 ** 6, 10 ** 4, replace=False).astype(np.uint64)
+    return ak, rng.uniform(-1, 1, 10 ** 4), bk, rng.uniform(-1, 1, 10 ** 4)
+
+
+def run_contraction(args):
+    """Plain sparse contraction, MIA level: toStraightLattice(a) (sort), toLatticeSort(b)
+    (re-key to {2,0,1} + sort), csc_no_accum, all through the C ABI."""
+    import torch
+
+    import libnt_b200 as L
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ak, av, bk, bv = contraction_inputs()
+    hk = [torch.from_numpy(x.view(np.int64) if x.dtype == np.uint64 else x).pin_memory() for x in (ak, av, bk, bv)]
+    dk = [torch.empty_like(x, device=dev) for x in hk]
+    dims = [100, 100, 100]
+    spec_a = L.RekeySpec.make(dims, [0, 1, 2], [0, 1, 2])
+    spec_b = L.RekeySpec.make(dims, [0, 1, 2], [2, 0, 1])
+    sa, sb = [torch.empty_like(x) for x in dk[:2]], [torch.empty_like(x) for x in dk[2:]]
+    ws = L.workspace(L.permute_sort_workspace(10 ** 4, 10 ** 6), dev)
+    out_h = [torch.empty(10 ** 4, dtype=torch.int64, pin_memory=True), torch.empty(10 ** 4, dtype=torch.float64,
+                                                                                    pin_memory=True)]
+
+    def step(host_io):
+        if host_io:
+            for d_, h_ in zip(dk, hk):
+                d_.copy_(h_, non_blocking=True)
+        L.permute_sort(dk[0], dk[1], max_key=10 ** 6, rekey=spec_a, out_keys=sa[0], out_vals=sa[1], ws=ws)
+        L.permute_sort(dk[2], dk[3], max_key=10 ** 6, rekey=spec_b, out_keys=sb[0], out_vals=sb[1], ws=ws)
+        ck, cv, prods = L.lattice_mult(sa[0], sa[1], sb[0], sb[1], 100, 10 ** 4, 100, 1)
+        if host_io:
+            out_h[0][:ck.numel()].copy_(ck)
+            out_h[1][:cv.numel()].copy_(cv)
+        return prods, ck.numel()
+
+    for _ in range(args.warmup):
+        prods, nc = step(True)
+    torch.cuda.synchronize()
+    launches0 = L.launch_count()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(args.steps):
+        step(False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    launches = L.launch_count() - launches0
+    f0, f1 = _events()
+    f0.record()
+    for _ in range(args.steps):
+        step(True)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+    if rank != 0:
+        return 0
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        t0 = time.perf_counter()
+        reps = 20
+        for _ in range(reps):
+            a = oracle.SparseMIA(dims, ak, av, sorted=False)
+            b = oracle.SparseMIA(dims, bk, bv, sorted=False)
+            if oracle.ref_available():
+                ka, va = oracle.ref_radix_sort(a.keys, a.vals, 10 ** 6)
+                kb, vb = oracle.ref_radix_sort(oracle.ref_rekey(b.keys, dims, [0, 1, 2], [2, 0, 1]), b.vals, 10 ** 6)
+            else:
+                ka, va = oracle.sort_pairs(a.keys, a.vals)
+                kb, vb = oracle.sort_pairs(oracle.rekey(b.keys, dims, [0, 1, 2], [2, 0, 1]), b.vals)
+            oracle.lattice_mult(ka, va, 100, 10 ** 4, 1, kb, vb, 100)
+        t = (time.perf_counter() - t0) / reps
+        cpu = {"value": prods / t, "unit": "products/s", "cores": 1,
+               "kind": "reference" if oracle.ref_available() else "port",
+               "sample": "the full workload, median-free mean of 20 runs: reference sorts + restated csc_no_accum"}
+    config = {"workload": "plain sparse contraction c(i,l)=a(i,j,k)*b(k,l,j), dims 100^3, 10^4 nnz each, "
+                          "seed 0, both unsorted (sort a, re-key+sort b, csc_no_accum)",
+              "products": prods, "output_nnz": nc, "l2": "inputs fit in L2 (latency-bound workload)"}
+    print(json.dumps(_line("products/s", prods * world / (ms * 1e-3), ms, args, world, config, {
+        "e2e": {"value": prods * world / (e2e_ms * 1e-3), "unit": "products/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": 4 * 8 * 10 ** 4, "d2h_bytes_per_step": 16 * nc + 16},
+        "gpu_launches": launches, "cpu_baseline": cpu,
+        "roofline": {"bound": "latency", "note": "about 0.5 MB of data: the step is launch- and latency-bound"},
+    })), flush=True)
+    return 0
+
+
+def batched_inputs(count=4096, seed=0):
+    """4096 problems a(i,j,k)*b(k,l,j) as lattices: dims U{16..512}, nnz log-uniform
+    in [1e2, 1e5] clamped to the lattice size, values U[-1,1], key-sorted sets."""
+    rng = np.random.default_rng(seed)
+    dims, ak, av, bk, bv = [], [], [], [], []
+    for p in range(count):
+        prng = np.random.default_rng([seed, p])
+        i, j, k, l = (int(x) for x in prng.integers(16, 513, 4))
+        h, w, wB = i, j * k, l
+        na = min(int(round(10 ** prng.uniform(2, 5))), h * w)
+        nb = min(int(round(10 ** prng.uniform(2, 5))), w * wB)
+        a = np.unique(prng.integers(0, h * w, int(na * 1.1) + 8, dtype=np.uint64))[:na]
+        b = np.unique(prng.integers(0, w * wB, int(nb * 1.1) + 8, dtype=np.uint64))[:nb]
+        dims.append((h, w, wB, 1))
+        ak.append(np.sort(prng.permutation(a)[:na]))
+        bk.append(np.sort(prng.permutation(b)[:nb]))
+        av.append(prng.uniform(-1, 1, ak[-1].size))
+        bv.append(prng.uniform(-1, 1, bk[-1].size))
+    a_off = np.concatenate([[0], np.cumsum([x.size for x in ak])]).astype(np.uint64)
+    b_off = np.concatenate([[0], np.cumsum([x.size for x in bk])]).astype(np.uint64)
+    return np.array(dims, np.int64), a_off, b_off, ak, av, bk, bv
+
+
+def run_batched(args):
+    import torch
+
+    import libnt_b200 as L
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dims, a_off, b_off, ak, av, bk, bv = batched_inputs(seed=rank)
+    cat = [np.concatenate(x) for x in (ak, av, bk, bv)]
+    dt = [torch.from_numpy(x.view(np.int64) if x.dtype == np.uint64 else x).to(dev) for x in cat]
+    batch = L.Batch(dims, a_off, b_off, *dt)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(args.warmup):
+            batch.run()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        batch.run()
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    launches0 = L.launch_count()
+    e0, e1 = _events()
+    sampler = ClockSampler(torch.cuda.current_device())
+    with sampler:
+        e0.record()
+        for _ in range(args.steps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    out_total = int(batch.c_off[-1].item())
+    # products per problem (for the metric): sum over B entries of the A column size
+    products = 0
+    for p in range(len(dims)):
+        h, w = int(dims[p][0]), int(dims[p][1])
+        acols = (ak[p] // h).astype(np.int64)
+        cnt = np.bincount(acols, minlength=w)
+        products += int(cnt[(bk[p] % w).astype(np.int64)].sum())
+    # per-contraction loop on the same device: plan + sync + mult, one problem at a time
+    loop_n = min(len(dims), 512)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lp = 0
+    for p in range(loop_n):
+        a0, a1, b0, b1 = int(a_off[p]), int(a_off[p + 1]), int(b_off[p]), int(b_off[p + 1])
+        h, w, wB, _ = (int(x) for x in dims[p])
+        _, _, pr = L.lattice_mult(dt[0][a0:a1], dt[1][a0:a1], dt[2][b0:b1], dt[3][b0:b1], h, w, wB, 1)
+        lp += pr
+    torch.cuda.synchronize()
+    loop_s = time.perf_counter() - t0
+    if rank != 0:
+        return 0
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        n_cpu = 256
+        t0 = time.perf_counter()
+        cp = 0
+        for p in range(n_cpu):
+            h, w, wB, _ = (int(x) for x in dims[p])
+            ck, cv = oracle.lattice_mult(ak[p], av[p], h, w, 1, bk[p], bv[p], wB)
+            acols = (ak[p] // h).astype(np.int64)
+            cp += int(np.bincount(acols, minlength=w)[(bk[p] % w).astype(np.int64)].sum())
+        t = time.perf_counter() - t0
+        cpu = {"value": cp / t, "unit": "products/s", "cores": 1, "kind": "port",
+               "sample": f"first {n_cpu} of the 4096 problems, restated csc_no_accum per problem (operands pre-sorted)"}
+    config = {"workload": "4096 independent lattice products a(i,j,k)*b(k,l,j): dims U{16..512}, nnz log-U[1e2,1e5] "
+                          "per operand, f64 U[-1,1]; one CUDA graph of the batched pipeline (persistent SPA kernels)",
+              "problems": len(dims), "products": products, "output_nnz": out_total,
+              "queue_chunk": os.environ.get("LNT_BATCH_CHUNK", "8")}
+    print(json.dumps(_line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
+        "per_contraction_loop": {"problems": loop_n, "ms": loop_s * 1e3,
+                                 "products_per_s": lp / loop_s,
+                                 "note": "lnt_lattice_mult_plan + count read-back + lnt_lattice_mult per problem"},
+        "gpu_launches": (L.launch_count() - launches0), "cpu_baseline": cpu, "clocks": sampler.summary(),
+        "roofline": {"bound": "latency/launch", "note": "small uneven problems; see per_contraction_loop"},
+    })), flush=True)
+    return 0
+
+
+def run_dense(args):
+    """c(i,j,m,n) = a(i,j,k,l) * b(k,l,m,n), all dims 128: a 16384^3 FP64 GEMM."""
+    import torch
+
+    import libnt_b200 as L
+    import oracle
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n = 1 << args.dense_log2
+    g = torch.Generator(device=dev)
+    g.manual_seed(5 + rank)
+    results = {}
+    for variant in ("uniform", "wide_exponent"):
+        slices = args.slices if variant == "uniform" else max(args.slices, 8)
+        if variant == "uniform":
+            A = torch.rand(n * n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+            B = torch.rand(n * n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+        else:
+            def wide():
+                m = torch.rand(n * n, generator=g, device=dev, dtype=torch.float64) + 1
+                e = torch.randint(-20, 21, (n * n,), generator=g, device=dev).to(torch.float64)
+                sgn = torch.randint(0, 2, (n * n,), generator=g, device=dev).to(torch.float64) * 2 - 1
+                return m * torch.pow(2.0, e) * sgn
+            A, B = wide(), wide()
+        ws = L.workspace(L.dense_split_workspace(n, n, n, slices), dev)
+        ws64 = L.workspace(64 << 20, dev)
+        Cs = torch.empty(n * n, dtype=torch.float64, device=dev)
+        C64 = torch.empty(n * n, dtype=torch.float64, device=dev)
+        for _ in range(max(1, args.warmup // 3)):
+            L.dense_mult_split(A, B, n, n, n, 1, slices, out=Cs, ws=ws)
+            L.dense_mult_fp64(A, B, n, n, n, 1, out=C64, ws=ws64)
+        torch.cuda.synchronize()
+        reps = max(1, min(args.steps, 5))
+        L.profile_reset()
+        L.profile_enable(True)
+        e0, e1 = _events()
+        sampler = ClockSampler(torch.cuda.current_device())
+        with sampler:
+            e0.record()
+            for _ in range(reps):
+                L.dense_mult_split(A, B, n, n, n, 1, slices, out=Cs, ws=ws)
+            e1.record()
+            torch.cuda.synchronize()
+        L.profile_enable(False)
+        t_split = e0.elapsed_time(e1) / reps
+        kern = {k: L.profile_query(k) for k in ("dense_split", "dense_int8_gemm", "dense_recombine")}
+        L.profile_reset()
+        f0, f1 = _events()
+        f0.record()
+        for _ in range(reps):
+            L.dense_mult_fp64(A, B, n, n, n, 1, out=C64, ws=ws64)
+        f1.record()
+        torch.cuda.synchronize()
+        t64 = f0.elapsed_time(f1) / reps
+        # error: sampled entries against compensated FP64 dots on the host
+        ns = 1024
+        rows = np.random.default_rng(1).integers(0, n, ns)
+        cols = np.random.default_rng(2).integers(0, n, ns)
+        Ah = A.cpu().numpy()
+        Bh = B.cpu().numpy()
+        ref, mag = oracle.dense_entries(Ah, Bh, n, n, rows, cols)
+        Csh = Cs.cpu().numpy()
+        C64h = C64.cpu().numpy()
+        idx = rows + n * cols
+        err_ab = float(np.max(np.abs(Csh[idx] - ref) / mag))
+        err_rel = float(np.max(np.abs(Csh[idx] - ref) / np.maximum(np.abs(ref), 1e-300)))
+        err64_ab = float(np.max(np.abs(C64h[idx] - ref) / mag))
+        full = float((Cs - C64).abs().max().item() / C64.abs().max().item())
+        flops = 2.0 * n ** 3
+        gemm_ms = kern["dense_int8_gemm"][0] / reps
+        int8_ops = sum((L_ + 1) for L_ in range(slices)) * 2.0 * n ** 3
+        results[variant] = {"slices": slices, "split_ms": t_split, "fp64_ms": t64, "speedup_vs_fp64": t64 / t_split,
+                            "effective_fp64_tflops": flops / (t_split * 1e-3) / 1e12,
+                            "fp64_tflops": flops / (t64 * 1e-3) / 1e12,
+                            "max_err_rel_absAabsB": err_ab, "max_err_rel_C": err_rel, "fp64_err_rel_absAabsB": err64_ab,
+                            "max_diff_vs_fp64_over_maxC": full, "sampled_entries": ns,
+                            "kernels_ms_per_step": {k: v[0] / reps for k, v in kern.items()},
+                            "int8_tensor_tops": int8_ops / (gemm_ms * 1e-3) / 1e12, "clocks": sampler.summary()}
+        del A, B, Cs, C64, ws
+        torch.cuda.empty_cache()
+    if rank != 0:
+        return 0
+    # INT8 tensor peak measured here (torch._int_mm 8192^3), the roofline denominator
+    a8 = torch.randint(-64, 64, (8192, 8192), device=dev, dtype=torch.int8)
+    b8 = torch.randint(-64, 64, (8192, 8192), device=dev, dtype=torch.int8)
+    for _ in range(3):
+        torch._int_mm(a8, b8)
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(10):
+        torch._int_mm(a8, b8)
+    e1.record()
+    torch.cuda.synchronize()
+    int8_peak = 2 * 8192 ** 3 / (e0.elapsed_time(e1) / 10 * 1e-3) / 1e12
+    u = results["uniform"]
+    config = {"workload": f"dense contraction c(i,j,m,n)=a(i,j,k,l)*b(k,l,m,n), dims 128 (a {n}^3 FP64 GEMM), "
+                          f"split into INT8 slices (7 for U[-1,1], 8 for 2^+-20 exponents), INT32 tensor products, "
+                          f"FP64 recombination",
+              "variants": results}
+    print(json.dumps(_line("TFLOP/s (FP64-equivalent)", u["effective_fp64_tflops"], u["split_ms"], args, world, config, {
+        "roofline": {"bound": "tensor", "kernel": "INT8 level GEMMs", "achieved": u["int8_tensor_tops"],
+                     "peak": int8_peak, "unit": "TOP/s", "frac": u["int8_tensor_tops"] / int8_peak,
+                     "peak_source": "int8 torch._int_mm 8192^3 measured in this run (MEASURED_PEAKS.json has bf16 only)"},
+        "vs_fp64_gemm": u["speedup_vs_fp64"], "clocks": u["clocks"],
+    })), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -373,12 +696,21 @@ def main():
     ap.add_argument("--nnz-log2", type=int, default=26,
                     help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
+    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense"],
+                    help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
+                         "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")
+    ap.add_argument("--slices", type=int, default=7, help="dense: INT8 slices per operand")
+    ap.add_argument("--dense-log2", type=int, default=14, help="dense: log2 of the GEMM size (14 = the workload)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
+        if args.workload != "merge":
+            print(json.dumps({"impl": "reference", "unavailable": "reference arm implemented for the merge workload"}))
+            return 0
         return run_reference(args)
-    return run_ours(args)
+    return {"merge": run_ours, "contraction": run_contraction, "batched": run_batched,
+            "dense": run_dense}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -242,6 +242,27 @@ LNT_API int lnt_batched_lattice_mult(int count, const int64_t* dims_host, const 
                                      void* workspace, size_t workspace_bytes, uint64_t* c_keys,
                                      double* c_vals, uint64_t* d_c_off, void* stream);
 
+/* ---- dense lattice product ---------------------------------------------- */
+
+/* C(:,:,t) = A(:,:,t) * B(:,:,t) for t < d; A is h x w, B is w x wB, C is
+ * h x wB, all float64 column-major, tabs stored one after another.  Replaces
+ * DenseLatticeBase::operator* (DenseLatticeBase.h:404-430, an Eigen GEMM per
+ * tab) as used by DenseMIA products (DenseMIA.h:200, 1240-1255).
+ * _fp64: plain float64 GEMM per tab (workspace from lnt_dense_fp64_workspace).
+ * _split: float64 operands split into `slices` signed 7-bit integer slices
+ * per row of A / column of B (power-of-two scaled), exact INT8 tensor-core
+ * products with INT32 accumulation, float64 recombination with compensated
+ * summation; error about 2^(-7 slices + 1) |A||B| per entry (slices = 7 for
+ * float64-class accuracy, <= 1e-12 relative).  Requires slices * w < 2^19. */
+LNT_API int lnt_dense_fp64_workspace(size_t* bytes);
+LNT_API int lnt_dense_lattice_mult_fp64(const double* A, const double* B, double* C, int64_t h,
+                                        int64_t w, int64_t wB, int64_t d, void* workspace,
+                                        size_t workspace_bytes, void* stream);
+LNT_API int lnt_dense_split_workspace(int64_t h, int64_t w, int64_t wB, int slices, size_t* bytes);
+LNT_API int lnt_dense_lattice_mult_split(const double* A, const double* B, double* C, int64_t h,
+                                         int64_t w, int64_t wB, int64_t d, int slices,
+                                         void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -91,6 +91,12 @@ _SIGS = {
     "lnt_batched_workspace": ([C.c_int, _vp, _vp, _vp, C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)], C.c_int),
     "lnt_batched_prepare": ([C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
     "lnt_batched_lattice_mult": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp], C.c_int),
+    "lnt_dense_fp64_workspace": ([C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_dense_lattice_mult_fp64": ([_vp, _vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _vp, _sz, _vp],
+                                    C.c_int),
+    "lnt_dense_split_workspace": ([C.c_int64, C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_dense_lattice_mult_split": ([_vp, _vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, _vp,
+                                      _sz, _vp], C.c_int),
 }
 
 _lib = None
@@ -378,3 +384,32 @@ class Batch:
     def result(self, p):
         off = self.c_off.tolist()
         return self.c_keys[off[p]:off[p + 1]], self.c_vals[off[p]:off[p + 1]]
+
+
+def dense_split_workspace(h: int, w: int, wB: int, slices: int = 7) -> int:
+    b = C.c_size_t(0)
+    _check(lib().lnt_dense_split_workspace(h, w, wB, slices, C.byref(b)), "lnt_dense_split_workspace")
+    return b.value
+
+
+def dense_mult_split(A, B, h: int, w: int, wB: int, d: int = 1, slices: int = 7, out=None, ws=None):
+    """Split-precision dense lattice product of column-major float64 A (h*w*d)
+    and B (w*wB*d); returns C (h*wB*d, column-major)."""
+    torch = _torch()
+    Cm = torch.empty(h * wB * d, dtype=torch.float64, device=A.device) if out is None else out
+    need = dense_split_workspace(h, w, wB, slices)
+    if ws is None or ws.numel() < need:
+        ws = workspace(need, A.device)
+    _check(lib().lnt_dense_lattice_mult_split(_ptr(A), _ptr(B), _ptr(Cm), h, w, wB, d, slices, _ptr(ws), ws.numel(),
+                                              _stream()), "lnt_dense_lattice_mult_split")
+    return Cm
+
+
+def dense_mult_fp64(A, B, h: int, w: int, wB: int, d: int = 1, out=None, ws=None):
+    torch = _torch()
+    Cm = torch.empty(h * wB * d, dtype=torch.float64, device=A.device) if out is None else out
+    if ws is None:
+        ws = workspace(64 << 20, A.device)
+    _check(lib().lnt_dense_lattice_mult_fp64(_ptr(A), _ptr(B), _ptr(Cm), h, w, wB, d, _ptr(ws), ws.numel(),
+                                             _stream()), "lnt_dense_lattice_mult_fp64")
+    return Cm

@@ -36,6 +36,10 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the LNT CUDA library cannot be built")
 
 
+def cuda_lib_dir() -> str:
+    return str(Path(nvcc()).resolve().parent.parent / "lib64")
+
+
 def _headers_mtime() -> float:
     hs = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h"))
     return max((h.stat().st_mtime for h in hs), default=0.0)
@@ -69,8 +73,8 @@ def build(verbose: bool = False, extra: list[str] | None = None, force: bool = F
                     print(f"[{obj.name}]\n{log}", file=sys.stderr)
     if force or todo or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static", "-lrt", "-ldl",
-               "-lpthread"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static", "-lcublasLt",
+               "-lrt", "-ldl", "-lpthread", "-Xlinker", f"-rpath={cuda_lib_dir()}"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

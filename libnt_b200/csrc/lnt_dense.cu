@@ -1,0 +1,360 @@
+// Dense lattice product C(:,:,t) = A(:,:,t) * B(:,:,t), column-major float64
+// (the reference's DenseLatticeBase::operator*, DenseLatticeBase.h:404-430: an
+// Eigen GEMM per tab), two ways:
+//
+// lnt_dense_lattice_mult_fp64: plain FP64 GEMM per tab (cuBLASLt DGEMM).
+//
+// lnt_dense_lattice_mult_split: error-free splitting onto the integer tensor
+// cores (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix
+// multiplication by using fast routines of matrix multiplication and its
+// applications", Numer. Algorithms 59 (2012), scheme I with integer slices):
+//   1. each row of A and each column of B is scaled by a power of two so its
+//      largest magnitude lies in [1/4, 1/2);
+//   2. every scaled entry x is split into s signed 7-bit digits,
+//      x = sum_p d_p 2^(-7(p+1)) + r, |d_p| <= 64, |r| <= 2^(-7s-1), all steps
+//      exact in float64 (x*128 - rint(x*128) is exact);
+//   3. the digit products d_p(A) d_q(B) are exact INT8 x INT8 -> INT32 tensor
+//      core products; all (p, q) with p + q = L are one GEMM over a K axis of
+//      (L+1) blocks (the slices of A are laid out [A_0|A_1|..] and those of B
+//      [B_{s-1}|..|B_0] along K, so each level reads a contiguous prefix /
+//      suffix); terms with p + q >= s lie below the kept precision and are
+//      dropped;
+//   4. one fused pass sums the s INT32 level results in float64 from the least
+//      significant level up, with Neumaier compensation, and applies the row
+//      and column scales.
+// With s = 7 (49 bits per operand) the error is about 2^-48 |A||B|
+// componentwise.  |d_p d_q| <= 2^12 and K' <= s*K keeps INT32 exact for
+// K <= 2^31 / (2^12 s) (74,898 at s = 7).
+#include <cublasLt.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "lnt_common.cuh"
+
+namespace lnt {
+namespace {
+
+constexpr int kDigitBits = 7;
+
+// ---- per-device cuBLASLt handle -------------------------------------------
+cublasLtHandle_t lt_handle() {
+  static std::mutex mu;
+  static cublasLtHandle_t handles[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> g(mu);
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!handles[dev]) cublasLtCreate(&handles[dev]);
+  return handles[dev];
+}
+
+// ---- scaling exponents ----------------------------------------------------
+// eA[i]: A row i's scale exponent (entries * 2^-eA lie in [-1/2, 1/2]).
+__global__ void row_exp_kernel(const double* __restrict__ A, u64 h, u64 w, int* __restrict__ eA) {
+  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= h) return;
+  double m = 0.0;
+  for (u64 k = 0; k < w; ++k) m = fmax(m, fabs(A[i + h * k]));
+  int e = 0;
+  if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [1/2, 1)
+  eA[i] = m > 0.0 ? e + 1 : 0;
+}
+
+// eB[j]: B column j's scale exponent; one warp per column.
+__global__ void col_exp_kernel(const double* __restrict__ B, u64 w, u64 wB, int* __restrict__ eB) {
+  const u64 j = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= wB) return;
+  double m = 0.0;
+  for (u64 k = lane; k < w; k += 32) m = fmax(m, fabs(B[k + w * j]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) {
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);
+    eB[j] = m > 0.0 ? e + 1 : 0;
+  }
+}
+
+// Splits x (already scaled into [-1/2, 1/2]) into s signed 7-bit digits.
+__device__ __forceinline__ void split_digits(double x, int s, signed char* out, size_t stride) {
+  for (int p = 0; p < s; ++p) {
+    x *= 128.0;
+    const double d = rint(x);
+    x -= d;
+    out[(size_t)p * stride] = (signed char)(int)d;
+  }
+}
+
+// A (h x w col-major) -> Acat: h rows of s*Kp int8, slice p at columns [p*Kp, p*Kp + w).
+// 32x32 tiles through shared memory: read coalesced along rows, write along K.
+__global__ void split_a_kernel(const double* __restrict__ A, u64 h, u64 w, u64 Kp, int s,
+                               const int* __restrict__ eA, signed char* __restrict__ Acat) {
+  __shared__ double tile[32][33];
+  const u64 i0 = (u64)blockIdx.x * 32, k0 = (u64)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const u64 i = i0 + tx, k = k0 + r;
+    tile[r][tx] = (i < h && k < w) ? A[i + h * k] : 0.0;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const u64 i = i0 + r, k = k0 + tx;
+    if (i < h && k < w) {
+      const double x = ldexp(tile[tx][r], -eA[i]);
+      split_digits(x, s, Acat + i * (u64)s * Kp + k, Kp);
+    }
+  }
+}
+
+// B (w x wB col-major) -> Bcat: wB rows of s*Kp int8, slice q at columns [(s-1-q)*Kp, ...).
+__global__ void split_b_kernel(const double* __restrict__ B, u64 w, u64 wB, u64 Kp, int s,
+                               const int* __restrict__ eB, signed char* __restrict__ Bcat) {
+  const u64 total = w * wB;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const u64 j = t / w, k = t - j * w;
+    const double x = ldexp(B[t], -eB[j]);
+    signed char* row = Bcat + j * (u64)s * Kp;
+    double y = x;
+    for (int q = 0; q < s; ++q) {
+      y *= 128.0;
+      const double d = rint(y);
+      y -= d;
+      row[(u64)(s - 1 - q) * Kp + k] = (signed char)(int)d;
+    }
+  }
+}
+
+// C[i + h j] = 2^(eA_i + eB_j) * sum_L 2^(-7(L+2)) lev[L][i + Mp j], summed
+// from the least significant level with Neumaier compensation.
+__global__ void recombine_kernel(const int* __restrict__ lev, u64 Mp, u64 Np, int s, u64 h, u64 wB,
+                                 const int* __restrict__ eA, const int* __restrict__ eB, double* __restrict__ C) {
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  const u64 mn = h * wB, plane = Mp * Np;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < mn; t += stride) {
+    const u64 j = t / h, i = t - j * h;
+    const u64 src = i + Mp * j;
+    double sum = 0.0, comp = 0.0;
+    for (int L = s - 1; L >= 0; --L) {
+      const double term = ldexp((double)lev[(u64)L * plane + src], -kDigitBits * (L + 2));
+      const double y = sum + term;
+      comp += fabs(sum) >= fabs(term) ? (sum - y) + term : (term - y) + sum;
+      sum = y;
+    }
+    C[t] = ldexp(sum + comp, eA[i] + eB[j]);
+  }
+}
+
+// The integer GEMMs run on M, N, K padded to multiples of 16 (the INT8
+// tensor-core GEMM needs 16-byte aligned leading dimensions); padding rows and
+// columns of the slice operands are zero.
+struct SplitLayout {
+  u64 Kp, Mp, Np;
+  size_t off_ea, off_eb, off_acat, off_bcat, off_lev, off_lt, lt_bytes, total;
+};
+
+SplitLayout split_layout(u64 h, u64 w, u64 wB, int s) {
+  SplitLayout L;
+  L.Kp = (w + 15) / 16 * 16;
+  L.Mp = (h + 15) / 16 * 16;
+  L.Np = (wB + 15) / 16 * 16;
+  size_t off = 0;
+  L.off_ea = off;
+  off += align_up(h * 4, 256);
+  L.off_eb = off;
+  off += align_up(wB * 4, 256);
+  L.off_acat = off;
+  off += align_up(L.Mp * (u64)s * L.Kp, 256);
+  L.off_bcat = off;
+  off += align_up(L.Np * (u64)s * L.Kp, 256);
+  L.off_lev = off;
+  off += align_up((u64)s * L.Mp * L.Np * 4, 256);
+  L.lt_bytes = 64ull << 20;
+  L.off_lt = off;
+  off += L.lt_bytes;
+  L.total = off;
+  return L;
+}
+
+int lt_int8_gemm(const signed char* A, int lda, const signed char* B, int ldb, int* C, u64 m, u64 n, u64 k,
+                 void* ltws, size_t ltws_bytes, cudaStream_t s) {
+  cublasLtHandle_t h = lt_handle();
+  if (!h) return LNT_DEVICE_ERROR;
+  cublasLtMatmulDesc_t op = nullptr;
+  cublasLtMatrixLayout_t la = nullptr, lb = nullptr, lc = nullptr;
+  cublasLtMatmulPreference_t pref = nullptr;
+  int st = LNT_DEVICE_ERROR;
+  do {
+    if (cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_32I, CUDA_R_32I) != CUBLAS_STATUS_SUCCESS) break;
+    cublasOperation_t ta = CUBLAS_OP_T, tb = CUBLAS_OP_N;
+    cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSA, &ta, sizeof(ta));
+    cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSB, &tb, sizeof(tb));
+    // A stored K x M (K-major rows of A), B stored K x N (K-major columns), C M x N
+    if (cublasLtMatrixLayoutCreate(&la, CUDA_R_8I, k, m, lda) != CUBLAS_STATUS_SUCCESS) break;
+    if (cublasLtMatrixLayoutCreate(&lb, CUDA_R_8I, k, n, ldb) != CUBLAS_STATUS_SUCCESS) break;
+    if (cublasLtMatrixLayoutCreate(&lc, CUDA_R_32I, m, n, m) != CUBLAS_STATUS_SUCCESS) break;
+    if (cublasLtMatmulPreferenceCreate(&pref) != CUBLAS_STATUS_SUCCESS) break;
+    cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &ltws_bytes,
+                                         sizeof(ltws_bytes));
+    cublasLtMatmulHeuristicResult_t res;
+    int found = 0;
+    if (cublasLtMatmulAlgoGetHeuristic(h, op, la, lb, lc, lc, pref, 1, &res, &found) != CUBLAS_STATUS_SUCCESS ||
+        !found) {
+      st = LNT_UNSUPPORTED;
+      break;
+    }
+    const int alpha = 1, beta = 0;
+    ProfScope prof("dense_int8_gemm", s);
+    if (cublasLtMatmul(h, op, &alpha, A, la, B, lb, &beta, C, lc, C, lc, &res.algo, ltws, ltws_bytes, s) !=
+        CUBLAS_STATUS_SUCCESS)
+      break;
+    st = LNT_OK;
+  } while (false);
+  if (pref) cublasLtMatmulPreferenceDestroy(pref);
+  if (lc) cublasLtMatrixLayoutDestroy(lc);
+  if (lb) cublasLtMatrixLayoutDestroy(lb);
+  if (la) cublasLtMatrixLayoutDestroy(la);
+  if (op) cublasLtMatmulDescDestroy(op);
+  return st;
+}
+
+int lt_dgemm(const double* A, const double* B, double* C, u64 m, u64 n, u64 k, void* ltws, size_t ltws_bytes,
+             cudaStream_t s) {
+  cublasLtHandle_t h = lt_handle();
+  if (!h) return LNT_DEVICE_ERROR;
+  cublasLtMatmulDesc_t op = nullptr;
+  cublasLtMatrixLayout_t la = nullptr, lb = nullptr, lc = nullptr;
+  cublasLtMatmulPreference_t pref = nullptr;
+  int st = LNT_DEVICE_ERROR;
+  do {
+    if (cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_64F, CUDA_R_64F) != CUBLAS_STATUS_SUCCESS) break;
+    if (cublasLtMatrixLayoutCreate(&la, CUDA_R_64F, m, k, m) != CUBLAS_STATUS_SUCCESS) break;
+    if (cublasLtMatrixLayoutCreate(&lb, CUDA_R_64F, k, n, k) != CUBLAS_STATUS_SUCCESS) break;
+    if (cublasLtMatrixLayoutCreate(&lc, CUDA_R_64F, m, n, m) != CUBLAS_STATUS_SUCCESS) break;
+    if (cublasLtMatmulPreferenceCreate(&pref) != CUBLAS_STATUS_SUCCESS) break;
+    cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &ltws_bytes,
+                                         sizeof(ltws_bytes));
+    cublasLtMatmulHeuristicResult_t res;
+    int found = 0;
+    if (cublasLtMatmulAlgoGetHeuristic(h, op, la, lb, lc, lc, pref, 1, &res, &found) != CUBLAS_STATUS_SUCCESS ||
+        !found) {
+      st = LNT_UNSUPPORTED;
+      break;
+    }
+    const double alpha = 1.0, beta = 0.0;
+    ProfScope prof("dense_dgemm", s);
+    if (cublasLtMatmul(h, op, &alpha, A, la, B, lb, &beta, C, lc, C, lc, &res.algo, ltws, ltws_bytes, s) !=
+        CUBLAS_STATUS_SUCCESS)
+      break;
+    st = LNT_OK;
+  } while (false);
+  if (pref) cublasLtMatmulPreferenceDestroy(pref);
+  if (lc) cublasLtMatrixLayoutDestroy(lc);
+  if (lb) cublasLtMatrixLayoutDestroy(lb);
+  if (la) cublasLtMatrixLayoutDestroy(la);
+  if (op) cublasLtMatmulDescDestroy(op);
+  return st;
+}
+
+int check_dense(int64_t h, int64_t w, int64_t wB, int64_t d) {
+  if (h <= 0 || w <= 0 || wB <= 0 || d <= 0) return LNT_BAD_DIMS;
+  if (h > (1ll << 31) || w > (1ll << 31) || wB > (1ll << 31)) return LNT_UNSUPPORTED;
+  return LNT_OK;
+}
+
+}  // namespace
+}  // namespace lnt
+
+using namespace lnt;
+
+extern "C" {
+
+int lnt_dense_split_workspace(int64_t h, int64_t w, int64_t wB, int slices, size_t* bytes) {
+  int st = check_dense(h, w, wB, 1);
+  if (st != LNT_OK) return st;
+  if (!bytes || slices < 1 || slices > 8) return LNT_BAD_ARG;
+  const u64 Kp = ((u64)w + 15) / 16 * 16;
+  if ((u64)slices * Kp * 4096ull >= (1ull << 31)) return LNT_UNSUPPORTED;  // INT32 exactness bound
+  *bytes = split_layout(h, w, wB, slices).total;
+  return LNT_OK;
+}
+
+int lnt_dense_lattice_mult_split(const double* A, const double* B, double* C, int64_t h, int64_t w, int64_t wB,
+                                 int64_t d, int slices, void* workspace, size_t workspace_bytes, void* stream) {
+  int st = check_dense(h, w, wB, d);
+  if (st != LNT_OK) return st;
+  if (!A || !B || !C) return LNT_BAD_ARG;
+  size_t need = 0;
+  st = lnt_dense_split_workspace(h, w, wB, slices, &need);
+  if (st != LNT_OK) return st;
+  if (!workspace || workspace_bytes < need || (uintptr_t)workspace % 256) return LNT_WORKSPACE;
+  const SplitLayout L = split_layout(h, w, wB, slices);
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  int* eA = reinterpret_cast<int*>(ws + L.off_ea);
+  int* eB = reinterpret_cast<int*>(ws + L.off_eb);
+  signed char* Acat = reinterpret_cast<signed char*>(ws + L.off_acat);
+  signed char* Bcat = reinterpret_cast<signed char*>(ws + L.off_bcat);
+  int* lev = reinterpret_cast<int*>(ws + L.off_lev);
+  cudaStream_t s = as_stream(stream);
+  const int sms = sm_count();
+  const u64 uh = h, uw = w, uwB = wB, Kp = L.Kp;
+  for (int64_t t = 0; t < d; ++t) {
+    const double* At = A + (u64)t * uh * uw;
+    const double* Bt = B + (u64)t * uw * uwB;
+    double* Ct = C + (u64)t * uh * uwB;
+    {
+      ProfScope prof("dense_split", s);
+      row_exp_kernel<<<(unsigned)((uh + 255) / 256), 256, 0, s>>>(At, uh, uw, eA);
+      col_exp_kernel<<<(unsigned)((uwB * 32 + 255) / 256), 256, 0, s>>>(Bt, uw, uwB, eB);
+      if (Kp != uw || L.Mp != uh || L.Np != uwB) {  // zero every padding row and column
+        if (cudaMemsetAsync(Acat, 0, L.Mp * (u64)slices * Kp, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+        if (cudaMemsetAsync(Bcat, 0, L.Np * (u64)slices * Kp, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+      }
+      split_a_kernel<<<dim3((unsigned)((uh + 31) / 32), (unsigned)((uw + 31) / 32)), dim3(32, 8), 0, s>>>(
+          At, uh, uw, Kp, slices, eA, Acat);
+      split_b_kernel<<<sms * 16, 256, 0, s>>>(Bt, uw, uwB, Kp, slices, eB, Bcat);
+      count_launch(4);
+    }
+    const int ld = (int)((u64)slices * Kp);
+    for (int lvl = 0; lvl < slices; ++lvl) {
+      // sum over p + q = lvl: A blocks [0, lvl], B blocks [slices-1-lvl, slices-1]
+      st = lt_int8_gemm(Acat, ld, Bcat + (u64)(slices - 1 - lvl) * Kp, ld, lev + (u64)lvl * L.Mp * L.Np, L.Mp, L.Np,
+                        (u64)(lvl + 1) * Kp, ws + L.off_lt, L.lt_bytes, s);
+      if (st != LNT_OK) return st;
+      count_launch();
+    }
+    {
+      ProfScope prof("dense_recombine", s);
+      recombine_kernel<<<sms * 16, 256, 0, s>>>(lev, L.Mp, L.Np, slices, uh, uwB, eA, eB, Ct);
+      count_launch();
+    }
+  }
+  return launch_status();
+}
+
+int lnt_dense_fp64_workspace(size_t* bytes) {
+  if (!bytes) return LNT_BAD_ARG;
+  *bytes = 64ull << 20;
+  return LNT_OK;
+}
+
+int lnt_dense_lattice_mult_fp64(const double* A, const double* B, double* C, int64_t h, int64_t w, int64_t wB,
+                                int64_t d, void* workspace, size_t workspace_bytes, void* stream) {
+  int st = check_dense(h, w, wB, d);
+  if (st != LNT_OK) return st;
+  if (!A || !B || !C) return LNT_BAD_ARG;
+  if (!workspace || workspace_bytes < (64ull << 20)) return LNT_WORKSPACE;
+  cudaStream_t s = as_stream(stream);
+  for (int64_t t = 0; t < d; ++t) {
+    st = lt_dgemm(A + (u64)t * h * w, B + (u64)t * w * wB, C + (u64)t * h * wB, h, wB, w, workspace,
+                  workspace_bytes, s);
+    if (st != LNT_OK) return st;
+    count_launch();
+  }
+  return LNT_OK;
+}
+
+}  // extern "C"

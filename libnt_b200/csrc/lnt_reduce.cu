@@ -74,9 +74,6 @@ __global__ void __launch_bounds__(128) lead_kernel(const u64* __restrict__ keys,
   }
 }
 
-__device__ __forceinline__ unsigned long long ld_volatile64(const unsigned long long* p) {
-  return *reinterpret_cast<const volatile unsigned long long*>(p);
-}
 __device__ __forceinline__ void st_volatile64(unsigned long long* p, unsigned long long v) {
   *reinterpret_cast<volatile unsigned long long*>(p) = v;
 }

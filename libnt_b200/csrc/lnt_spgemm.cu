@@ -108,7 +108,7 @@ struct Identity64 {
 // ---- ESC engine ----------------------------------------------------------
 __global__ void expand_kernel(Lat A, Lat B, AColumns ac, const u64* __restrict__ boff, u64 P, Divider div_w,
                               Divider div_wB, u64* __restrict__ pk, double* __restrict__ pv) {
-  const u64 h = A.rows, w = A.cols, wB = B.cols;
+  const u64 h = A.rows, w = A.cols;
   const u64 stride = (u64)gridDim.x * blockDim.x;
   for (u64 p = (u64)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += stride) {
     // B entry e with boff[e] <= p < boff[e+1]

@@ -1,0 +1,73 @@
+"""GPU dense lattice products (DenseLatticeBase::operator*): the plain FP64
+path and the split-precision INT8 tensor-core path against the reference's
+golden fixture, its closed-form known answer and the oracle's compensated
+FP64 entries."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from test_gpu_sort import to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    return t
+
+
+def test_golden_fixture_fp64_and_split(cuda, torch):
+    """data/test1.bin x data/test2.bin = data/multtest_ddd.bin (5x5x10)."""
+    z = np.load(GOLDEN / "dense_lattice_5x5x10.npz")
+    h, w, wB, d = (int(x) for x in z["shape"])
+    A, B = to_dev(z["A"], torch), to_dev(z["B"], torch)
+    mag = np.abs(oracle.dense_lattice_mult(np.abs(z["A"]), np.abs(z["B"]), h, w, wB, d))
+    # the fixture is Eigen's summation order; a fused-multiply-add GEMM may differ by a rounding
+    c64 = to_host(cuda.dense_mult_fp64(A, B, h, w, wB, d))
+    assert np.all(np.abs(c64 - z["C"]) <= 4 * 2.0 ** -52 * mag)
+    cs = to_host(cuda.dense_mult_split(A, B, h, w, wB, d, slices=7))
+    assert np.all(np.abs(cs - z["C"]) <= 1e-13 * mag)
+
+
+def test_closed_form_kat_exact(cuda, torch):
+    """dense_mia_mult_test.cpp:44-74: a increments along the inner modes, b = 1:
+    every entry is dim2^2 (dim2^2 + 1) / 2 exactly on both paths."""
+    dim1, dim2 = 3, 4
+    h, w, wB = dim1 * dim1, dim2 * dim2, dim1 * dim1
+    A = np.empty((h, w))
+    A[:, :] = np.arange(1, w + 1)[None, :]
+    B = np.ones((w, wB))
+    Ad, Bd = to_dev(A.ravel(order="F"), torch), to_dev(B.ravel(order="F"), torch)
+    for Cm in (cuda.dense_mult_fp64(Ad, Bd, h, w, wB), cuda.dense_mult_split(Ad, Bd, h, w, wB)):
+        assert np.all(to_host(Cm) == w * (w + 1) / 2)
+
+
+# componentwise bound on |C - C_ref| / (|A||B|): uniform data loses nothing to the
+# row/column scaling; data spanning 2^+-20 inside a row keeps fewer bits in its
+# small entries, one more slice (7 more bits) restores them
+TOL = {("uniform", 7): 1e-13, ("uniform", 8): 1e-13, ("wide_exponent", 7): 2e-11, ("wide_exponent", 8): 1e-13}
+
+
+@pytest.mark.parametrize("h,w,wB,d", [(100, 300, 70, 3), (257, 1000, 129, 1), (64, 4096, 64, 1)])
+@pytest.mark.parametrize("variant", ["uniform", "wide_exponent"])
+@pytest.mark.parametrize("slices", [7, 8])
+def test_split_error_vs_compensated_fp64(cuda, torch, rng, h, w, wB, d, variant, slices):
+    if variant == "uniform":
+        A = rng.uniform(-1, 1, h * w * d)
+        B = rng.uniform(-1, 1, w * wB * d)
+    else:  # mantissa U[1,2) * 2^e, e in [-20, 20], random sign
+        A = rng.uniform(1, 2, h * w * d) * 2.0 ** rng.integers(-20, 21, h * w * d) * rng.choice([-1, 1], h * w * d)
+        B = rng.uniform(1, 2, w * wB * d) * 2.0 ** rng.integers(-20, 21, w * wB * d) * rng.choice([-1, 1], w * wB * d)
+    Cs = to_host(cuda.dense_mult_split(to_dev(A, torch), to_dev(B, torch), h, w, wB, d, slices=slices))
+    for t in range(d):
+        At = A[t * h * w:(t + 1) * h * w]
+        Bt = B[t * w * wB:(t + 1) * w * wB]
+        rows, cols = np.meshgrid(np.arange(h), np.arange(wB), indexing="ij")
+        ref, mag = oracle.dense_entries(At, Bt, h, w, rows.ravel(), cols.ravel())
+        got = Cs[t * h * wB:(t + 1) * h * wB].reshape(wB, h).T.ravel()
+        err = np.abs(got - ref) / np.maximum(mag, 1e-300)
+        assert err.max() <= TOL[(variant, slices)], err.max()
