@@ -119,6 +119,23 @@ LNT_API int lnt_sort_pairs(const uint64_t* keys_in, const double* vals_in,
 LNT_API int lnt_sort_variant_count(void);
 LNT_API int lnt_sort_variant(int index, int* bits, int* threads, int* items, int* window);
 
+/* Largest pair count lnt_sort_pairs_noalloc accepts. */
+#define LNT_SORT_NOALLOC_MAX_PAIRS 262144
+
+/* lnt_sort_pairs for callers that cannot allocate device memory (a stream
+ * being captured into a CUDA graph, a loop that must not synchronise on an
+ * allocation, a plugin with no device allocator).  No counterpart in the
+ * reference, whose sort needs no workspace.  Same result as lnt_sort_pairs,
+ * out of place only (LNT_BAD_ARG if an output aliases an input); at most
+ * LNT_SORT_NOALLOC_MAX_PAIRS pairs (else LNT_UNSUPPORTED).  Its scratch is one
+ * fixed 6 MiB array in device memory that every device loading this library
+ * holds until exit; calls share it, so calls whose GPU work overlaps race --
+ * order them on one stream.  The first call on a device looks the array up,
+ * so make it before any stream capture.  Allocates nothing. */
+LNT_API int lnt_sort_pairs_noalloc(const uint64_t* keys_in, const double* vals_in,
+                                   uint64_t* keys_out, double* vals_out, size_t n,
+                                   uint64_t max_key, void* stream);
+
 /* ---- duplicate collection ----------------------------------------------- */
 
 LNT_API int lnt_collect_duplicates_workspace(size_t n, size_t* bytes);

@@ -72,6 +72,7 @@ _SIGS = {
     "lnt_sort_variant_count": ([], C.c_int),
     "lnt_sort_variant": ([C.c_int] + [C.POINTER(C.c_int)] * 4, C.c_int),
     "lnt_sort_pairs_workspace": ([_sz, C.c_uint64, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_sort_pairs_noalloc": ([_vp, _vp, _vp, _vp, _sz, C.c_uint64, _vp], C.c_int),
     "lnt_sort_pairs": ([_vp, _vp, _vp, _vp, _sz, C.c_uint64, _vp, _sz, _vp], C.c_int),
     "lnt_collect_duplicates_workspace": ([_sz, C.POINTER(C.c_size_t)], C.c_int),
     "lnt_collect_duplicates": ([_vp, _vp, _sz, C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
