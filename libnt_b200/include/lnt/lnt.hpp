@@ -1,0 +1,712 @@
+// lnt.hpp - header-only C++17 front end of the LibNT B200 hot path.
+//
+// Mirrors the reference's index-label operator API (MIA.h:222-238,
+// MIA_Expr.h, Index.h): sparse and dense multi-index arrays addressed with
+// index labels,
+//
+//     lnt::Index i, j, k, l;
+//     c(i, l) = a(i, j, k) * b(k, l, j);        // lattice contraction
+//     c4(i, j, k, l) = a4(i, j, k, l) + b4(l, k, j, i);   // merge under permutation
+//     d(i, l, !n) = a(i, j, !n) * b(j, l, !n);  // element-wise index (a tab)
+//
+// with the same results and the same side effects on the operands as the
+// reference: operands are re-keyed / re-sorted in place exactly where the
+// reference does it (sortMerge, outside_scanMerge, toStraightLattice,
+// toLatticeSort), linIdxSequence() and is_sorted() follow the reference's
+// rules, and assignment to a differently ordered target only relabels.
+//
+// All arithmetic runs on the current CUDA device through the C ABI of
+// include/lnt.h; tensors own device buffers.  Labels are run-time objects
+// (the reference resolves them at compile time with Boost.MPL); the
+// classification into outer / inner / element-wise modes follows
+// solve_product_expr_helper (MIA_Expr.h:449-529).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "lnt.h"
+
+namespace lnt {
+
+// ---- errors (the reference's exception names, LibMIAException.h:25-92) ----
+struct LibMIAException : std::runtime_error {
+  explicit LibMIAException(const std::string& m) : std::runtime_error(m) {}
+};
+struct DimensionMismatchException : LibMIAException {
+  using LibMIAException::LibMIAException;
+};
+struct MIAParameterException : LibMIAException {
+  using LibMIAException::LibMIAException;
+};
+struct LatticeParameterException : LibMIAException {
+  using LibMIAException::LibMIAException;
+};
+struct DeviceException : LibMIAException {
+  using LibMIAException::LibMIAException;
+};
+
+inline void check(int st, const char* what) {
+  if (st == LNT_OK) return;
+  std::string m = std::string(what) + ": " + lnt_status_string(st);
+  if (st == LNT_BAD_DIMS) throw DimensionMismatchException(m);
+  if (st == LNT_BAD_ARG || st == LNT_BAD_SEQ || st == LNT_OVERFLOW_KEYBITS) throw MIAParameterException(m);
+  throw DeviceException(m);
+}
+
+inline void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw DeviceException(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---- device memory ----------------------------------------------------------
+template <class T>
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(size_t n) { resize(n); }
+  DeviceBuffer(const DeviceBuffer& o) { *this = o; }
+  DeviceBuffer& operator=(const DeviceBuffer& o) {
+    if (this != &o) {
+      resize(o.n_);
+      if (o.n_) cuda_check(cudaMemcpy(p_, o.p_, o.n_ * sizeof(T), cudaMemcpyDeviceToDevice), "copy");
+    }
+    return *this;
+  }
+  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_), cap_(o.cap_) { o.p_ = nullptr, o.n_ = o.cap_ = 0; }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    std::swap(p_, o.p_), std::swap(n_, o.n_), std::swap(cap_, o.cap_);
+    return *this;
+  }
+  ~DeviceBuffer() {
+    if (p_) cudaFree(p_);
+  }
+  void resize(size_t n) {  // contents are not preserved when growing
+    if (n > cap_) {
+      if (p_) cudaFree(p_);
+      p_ = nullptr;
+      cuda_check(cudaMalloc(&p_, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+      cap_ = n;
+    }
+    n_ = n;
+  }
+  void shrink(size_t n) { n_ = std::min(n, n_); }  // keep contents, drop the tail
+  T* data() { return p_; }
+  const T* data() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  T* p_ = nullptr;
+  size_t n_ = 0, cap_ = 0;
+};
+
+// Grow-only scratch shared by operations on this thread.
+inline void* scratch(size_t bytes) {
+  thread_local DeviceBuffer<unsigned char> buf;
+  if (buf.size() < bytes) buf.resize(bytes);
+  return buf.data();
+}
+
+inline uint64_t read_u64(const uint64_t* d) {
+  uint64_t h = 0;
+  cuda_check(cudaMemcpy(&h, d, 8, cudaMemcpyDeviceToHost), "read count");
+  return h;
+}
+
+// ---- index labels -------------------------------------------------------------
+// An index label (MIAINDEX / NTINDEX, Index.h:28-30); !i marks it element-wise
+// (Index.h:54-57).  Each label object has its own identity.
+class Index {
+ public:
+  Index() : id_(next_id()), elem_(false) {}
+  Index operator!() const { return Index(id_, !elem_); }
+  int id() const { return id_; }
+  bool elementwise() const { return elem_; }
+  bool operator==(const Index& o) const { return id_ == o.id_ && elem_ == o.elem_; }
+  bool same_id(const Index& o) const { return id_ == o.id_; }
+
+ private:
+  Index(int id, bool e) : id_(id), elem_(e) {}
+  static int next_id() {
+    static std::atomic<int> n{0};
+    return n++;
+  }
+  int id_;
+  bool elem_;
+};
+using Labels = std::vector<Index>;
+
+// ---- sparse tensors ------------------------------------------------------------
+// Run-time-order sparse multi-index array (SparseMIA<double, N> with N known
+// at run time): LCO storage on the device, linIdxSequence, sorted flag.
+class SparseTensor {
+ public:
+  SparseTensor() = default;
+  explicit SparseTensor(std::vector<int64_t> dims) : dims_(std::move(dims)), seq_(dims_.size()) {
+    std::iota(seq_.begin(), seq_.end(), 0);
+    for (auto d : dims_)
+      if (d <= 0) throw MIAParameterException("dimensions must be positive");
+  }
+
+  // Host upload: keys linearised under `seq` (default sequence if empty).
+  void assign_host(const std::vector<uint64_t>& keys, const std::vector<double>& vals, bool is_sorted,
+                   std::vector<int> seq = {}) {
+    if (keys.size() != vals.size()) throw MIAParameterException("keys and values differ in length");
+    keys_.resize(keys.size());
+    vals_.resize(vals.size());
+    if (!keys.empty()) {
+      cuda_check(cudaMemcpy(keys_.data(), keys.data(), keys.size() * 8, cudaMemcpyHostToDevice), "upload");
+      cuda_check(cudaMemcpy(vals_.data(), vals.data(), vals.size() * 8, cudaMemcpyHostToDevice), "upload");
+    }
+    if (!seq.empty()) seq_ = std::move(seq);
+    sorted_ = is_sorted;
+  }
+  void download(std::vector<uint64_t>& keys, std::vector<double>& vals) const {
+    keys.resize(size());
+    vals.resize(size());
+    if (size()) {
+      cuda_check(cudaMemcpy(keys.data(), keys_.data(), size() * 8, cudaMemcpyDeviceToHost), "download");
+      cuda_check(cudaMemcpy(vals.data(), vals_.data(), size() * 8, cudaMemcpyDeviceToHost), "download");
+    }
+  }
+
+  size_t order() const { return dims_.size(); }
+  const std::vector<int64_t>& dims() const { return dims_; }
+  int64_t dim(size_t i) const { return dims_[i]; }
+  const std::vector<int>& linIdxSequence() const { return seq_; }
+  bool is_sorted() const { return sorted_; }
+  void setSorted(bool s) { sorted_ = s; }
+  size_t size() const { return keys_.size(); }
+  uint64_t dimensionality() const {
+    uint64_t d = 1;
+    for (auto x : dims_) d *= (uint64_t)x;
+    return d;
+  }
+  uint64_t* keys() { return keys_.data(); }
+  double* vals() { return vals_.data(); }
+  const uint64_t* keys() const { return keys_.data(); }
+  const double* vals() const { return vals_.data(); }
+
+  // SparseMIABase::change_linIdx_sequence (SparseMIABase.h:768-814)
+  void change_linIdx_sequence(const std::vector<int>& seq) {
+    if (seq == seq_ || order() == 1) return;
+    if (size()) {
+      check(lnt_rekey(keys(), keys(), size(), (int)order(), dims_.data(), seq_.data(), seq.data(), nullptr),
+            "change_linIdx_sequence");
+    }
+    seq_ = seq;
+    sorted_ = false;
+  }
+
+  // SparseMIABase::sort() (SparseMIABase.h:701-734)
+  void sort() {
+    if (!sorted_ && size()) sort_keys_();
+    sorted_ = true;
+  }
+
+  // SparseMIABase::sort(seq) (SparseMIABase.h:590-645)
+  void sort(const std::vector<int>& seq) {
+    if (!sorted_) {
+      change_linIdx_sequence(seq);
+      sort();
+    } else if (order() != 1 && seq != seq_) {
+      change_linIdx_sequence(seq);
+      if (size()) sort_keys_();
+      if (size() < 3000) {  // the introsort branch returns before setSorted(true)
+        sorted_ = false;
+        return;
+      }
+      sorted_ = true;
+    } else {
+      sorted_ = true;
+    }
+  }
+
+  // SparseMIA::collect_duplicates(std::plus) (SparseMIA.h:636-665)
+  void collect_duplicates() {
+    if (!size()) {
+      sorted_ = true;
+      return;
+    }
+    const size_t n = size();
+    DeviceBuffer<uint64_t> k(n);
+    DeviceBuffer<double> v(n);
+    DeviceBuffer<uint64_t> cnt(1);
+    size_t need = 0;
+    check(lnt_sort_reduce_workspace(n, 0, dimensionality(), &need), "collect_duplicates");
+    if (sorted_) {
+      check(lnt_collect_duplicates_workspace(n, &need), "collect_duplicates");
+      check(lnt_collect_duplicates(keys(), vals(), n, 1, k.data(), v.data(), cnt.data(), scratch(need), need,
+                                   nullptr),
+            "collect_duplicates");
+    } else {
+      check(lnt_sort_reduce(keys(), vals(), n, nullptr, nullptr, nullptr, 0, nullptr, 1.0, dimensionality(), 1,
+                            k.data(), v.data(), cnt.data(), scratch(need), need, nullptr),
+            "collect_duplicates");
+    }
+    const uint64_t m = read_u64(cnt.data());
+    k.shrink(m);
+    v.shrink(m);
+    keys_ = std::move(k);
+    vals_ = std::move(v);
+    sorted_ = true;
+  }
+
+  // internal: replace storage
+  void take(DeviceBuffer<uint64_t>&& k, DeviceBuffer<double>&& v) {
+    keys_ = std::move(k);
+    vals_ = std::move(v);
+  }
+  void set_seq(std::vector<int> s) { seq_ = std::move(s); }
+  void set_dims(std::vector<int64_t> d) { dims_ = std::move(d); }
+
+ private:
+  void sort_keys_() {
+    const size_t n = size();
+    DeviceBuffer<uint64_t> k(n);
+    DeviceBuffer<double> v(n);
+    size_t need = 0;
+    check(lnt_permute_sort_workspace(n, dimensionality(), &need), "sort");
+    check(lnt_permute_sort(keys(), vals(), n, nullptr, k.data(), v.data(), dimensionality(), scratch(need), need,
+                           nullptr),
+          "sort");
+    keys_ = std::move(k);
+    vals_ = std::move(v);
+  }
+
+  std::vector<int64_t> dims_;
+  std::vector<int> seq_;
+  bool sorted_ = true;  // the dims-only constructor's default (SparseMIABase.h:220)
+  DeviceBuffer<uint64_t> keys_;
+  DeviceBuffer<double> vals_;
+};
+
+// ---- expression layer ---------------------------------------------------------
+namespace detail {
+
+inline std::vector<int> reverse_order(const std::vector<int>& o) {  // IndexUtil.h:893-914
+  std::vector<int> r(o.size(), (int)o.size());
+  for (size_t i = 0; i < o.size(); ++i)
+    for (size_t j = 0; j < o.size(); ++j)
+      if (o[j] == (int)i) {
+        r[i] = (int)j;
+        break;
+      }
+  return r;
+}
+
+inline std::vector<int> reorder_from(const std::vector<int>& from, const std::vector<int>& seq) {  // IndexUtil.h:231-252
+  std::vector<int> r(seq.size());
+  for (size_t i = 0; i < seq.size(); ++i) r[i] = from[seq[i]];
+  return r;
+}
+
+// pull_match_order (ExprUtil.h:511-562): position of every left label in the right operand
+inline std::vector<int> match_order(const Labels& l, const Labels& r) {
+  if (l.size() != r.size()) throw MIAParameterException("operands of a merge must have the same order");
+  std::vector<int> o(l.size());
+  for (size_t i = 0; i < l.size(); ++i) {
+    int pos = -1;
+    for (size_t j = 0; j < r.size(); ++j)
+      if (r[j] == l[i]) pos = (int)j;
+    if (pos < 0) throw MIAParameterException("merge operands must carry the same index labels");
+    o[i] = pos;
+  }
+  return o;
+}
+
+struct ProductOrders {
+  std::vector<int> l_outer, l_inner, l_inter, r_outer, r_inner, r_inter;
+};
+
+// solve_product_expr_helper (MIA_Expr.h:449-529) over pull_left_operand_index_sequence
+// (ExprUtil.h:311-393) and pull_right_index_order (ExprUtil.h:564-645)
+inline ProductOrders product_orders(const Labels& l, const Labels& r) {
+  ProductOrders o;
+  for (size_t i = 0; i < l.size(); ++i) {
+    int n = 0, same_id = 0;
+    for (const auto& x : r) {
+      n += (x == l[i]);
+      same_id += x.same_id(l[i]);
+    }
+    if (n > 1) throw MIAParameterException("index repeated in an operand");
+    if (n == 0 && same_id) throw MIAParameterException("an index appears with different element-wise marks");
+    if (n == 0)
+      o.l_outer.push_back((int)i);
+    else if (l[i].elementwise())
+      o.l_inter.push_back((int)i);
+    else
+      o.l_inner.push_back((int)i);
+  }
+  auto find = [&](const Index& x) {
+    for (size_t j = 0; j < r.size(); ++j)
+      if (r[j] == x) return (int)j;
+    return -1;
+  };
+  for (size_t j = 0; j < r.size(); ++j) {
+    bool in_l = false;
+    for (const auto& x : l) in_l = in_l || x == r[j];
+    if (!in_l) o.r_outer.push_back((int)j);
+  }
+  for (int i : o.l_inner) o.r_inner.push_back(find(l[i]));
+  for (int i : o.l_inter) o.r_inter.push_back(find(l[i]));
+  return o;
+}
+
+inline uint64_t prod_dims(const SparseTensor& m, const std::vector<int>& modes) {
+  uint64_t p = 1;
+  for (int i : modes) p *= (uint64_t)m.dim(i);
+  return p;
+}
+
+// toStraightLattice / toLatticeSort (SparseMIABase.h:1457-1586), column major:
+// sort under rows+cols+tabs and clear the sorted flag.
+inline void to_lattice(SparseTensor& m, const std::vector<int>& rows, const std::vector<int>& cols,
+                       const std::vector<int>& tabs) {
+  std::vector<int> seq = rows;
+  seq.insert(seq.end(), cols.begin(), cols.end());
+  seq.insert(seq.end(), tabs.begin(), tabs.end());
+  m.sort(seq);
+  m.setSorted(false);
+}
+
+}  // namespace detail
+
+struct SparseAtom;
+
+// The result of an expression: an owned tensor and its labels.
+struct SparseExpr {
+  SparseTensor t;
+  Labels labels;
+};
+
+// a(i, j, k): a tensor viewed with labels (MIA_Atom, MIA_Expr.h:738-1400).
+struct SparseAtom {
+  SparseTensor* m;
+  Labels labels;
+
+  // c(...) = expression: relabel only (SparseMIA::assign, SparseMIA.h:891-928)
+  SparseAtom& operator=(SparseExpr&& e) {
+    if (e.labels.size() != labels.size()) throw MIAParameterException("assignment between different orders");
+    if (e.labels == labels) {
+      *m = std::move(e.t);
+      return *this;
+    }
+    const std::vector<int> index_order = detail::match_order(labels, e.labels);
+    std::vector<int64_t> nd(labels.size());
+    for (size_t i = 0; i < labels.size(); ++i) nd[i] = e.t.dim(index_order[i]);
+    const std::vector<int> lhs = detail::reverse_order(index_order);
+    std::vector<int> nseq(labels.size());
+    for (size_t i = 0; i < labels.size(); ++i) nseq[i] = lhs[e.t.linIdxSequence()[i]];
+    e.t.set_dims(nd);
+    e.t.set_seq(nseq);
+    *m = std::move(e.t);
+    return *this;
+  }
+  SparseAtom& operator=(const SparseAtom& o) {
+    SparseExpr e{*o.m, o.labels};
+    return *this = std::move(e);
+  }
+  SparseAtom& operator+=(const SparseAtom& o);
+  SparseAtom& operator-=(const SparseAtom& o);
+};
+
+namespace detail {
+
+// SparseMIA::sortMerge (SparseMIA.h:833-887): C is a copy of A; both unsorted.
+inline void sort_merge(SparseTensor& c, SparseTensor& b, const std::vector<int>& index_order, int op) {
+  lnt_rekey_spec spec{};
+  const lnt_rekey_spec* a_spec = nullptr;
+  const lnt_rekey_spec* b_spec = nullptr;
+  std::vector<int> new_seq;
+  const SparseTensor* rekeyed = nullptr;
+  if (c.size() > b.size()) {
+    new_seq = reorder_from(index_order, c.linIdxSequence());  // b into c's order; b itself is re-keyed
+    b.change_linIdx_sequence(new_seq);
+  } else {
+    new_seq = reorder_from(reverse_order(index_order), b.linIdxSequence());
+    rekeyed = &c;
+  }
+  if (rekeyed) {  // fused: c re-keyed inside the sort's first pass
+    spec.order = (int32_t)c.order();
+    for (size_t i = 0; i < c.order(); ++i) {
+      spec.cur_seq[i] = c.linIdxSequence()[i];
+      spec.new_seq[i] = new_seq[i];
+      spec.dims[i] = c.dim(i);
+    }
+    a_spec = &spec;
+  }
+  const size_t na = c.size(), nb = b.size(), n = na + nb;
+  DeviceBuffer<uint64_t> k(std::max<size_t>(n, 1));
+  DeviceBuffer<double> v(std::max<size_t>(n, 1));
+  DeviceBuffer<uint64_t> cnt(1);
+  size_t need = 0;
+  check(lnt_sort_reduce_workspace(na, nb, c.dimensionality(), &need), "merge");
+  check(lnt_sort_reduce(c.keys(), c.vals(), na, a_spec, b.keys(), b.vals(), nb, b_spec, op == 1 ? -1.0 : 1.0,
+                        c.dimensionality(), 1, k.data(), v.data(), cnt.data(), scratch(need), need, nullptr),
+        "merge");
+  const uint64_t m = read_u64(cnt.data());
+  k.shrink(m);
+  v.shrink(m);
+  if (rekeyed) c.set_seq(new_seq);
+  c.take(std::move(k), std::move(v));
+  c.setSorted(true);
+}
+
+// SparseMIABase::outside_scanMerge (SparseMIABase.h:1404-1455)
+inline SparseTensor scan_merge(SparseTensor& a, SparseTensor& b, const std::vector<int>& index_order, int op) {
+  if (b.is_sorted() && !a.is_sorted()) {
+    a.sort(reorder_from(reverse_order(index_order), b.linIdxSequence()));
+  } else if (a.is_sorted() && !b.is_sorted()) {
+    b.sort(reorder_from(index_order, a.linIdxSequence()));
+  } else if (b.size() < a.size()) {
+    b.sort(reorder_from(index_order, a.linIdxSequence()));
+  } else {
+    a.sort(reorder_from(reverse_order(index_order), b.linIdxSequence()));
+  }
+  SparseTensor c(a.dims());
+  c.change_linIdx_sequence(a.linIdxSequence());  // empty: sets the sequence, clears the flag if it differs
+  const size_t n = a.size() + b.size();
+  DeviceBuffer<uint64_t> k(std::max<size_t>(n, 1));
+  DeviceBuffer<double> v(std::max<size_t>(n, 1));
+  DeviceBuffer<uint64_t> cnt(1);
+  size_t need = 0;
+  check(lnt_merge_sorted_workspace(a.size(), b.size(), &need), "merge");
+  check(lnt_merge_sorted(a.keys(), a.vals(), a.size(), b.keys(), b.vals(), b.size(), op, k.data(), v.data(),
+                         cnt.data(), scratch(need), need, nullptr),
+        "merge");
+  const uint64_t m = read_u64(cnt.data());
+  k.shrink(m);
+  v.shrink(m);
+  c.take(std::move(k), std::move(v));
+  return c;
+}
+
+// perform_outside_merge (SparseMIABase.h:1377-1402)
+inline SparseExpr merge(SparseAtom& a, SparseAtom& b, int op) {
+  const std::vector<int> order = match_order(a.labels, b.labels);
+  for (size_t i = 0; i < order.size(); ++i)
+    if (a.m->dim(i) != b.m->dim(order[i])) throw DimensionMismatchException("merge dimension mismatch");
+  SparseTensor bcopy;
+  SparseTensor* bp = b.m;
+  if (a.m == b.m) {  // self-merge: merge with a copy (SparseMIABase.h:1368-1372)
+    bcopy = *b.m;
+    bp = &bcopy;
+  }
+  if (a.m->is_sorted() || bp->is_sorted()) return {scan_merge(*a.m, *bp, order, op), a.labels};
+  SparseTensor c = *a.m;
+  sort_merge(c, *bp, order, op);
+  return {std::move(c), a.labels};
+}
+
+// MIA_Atom::operator* for the lattice case (MIA_Expr.h:864-925) -> csc_no_accum.
+inline SparseExpr product(SparseAtom& a, SparseAtom& b) {
+  const ProductOrders o = product_orders(a.labels, b.labels);
+  if (o.l_inner.empty()) throw MIAParameterException("outer/element-wise-only products are not on this path");
+  SparseTensor bcopy;
+  SparseTensor* bp = b.m;
+  if (a.m == b.m) {  // check_if_copy_needed (MIA_Expr.h:767-802)
+    bcopy = *b.m;
+    bp = &bcopy;
+  }
+  for (size_t q = 0; q < o.l_inner.size(); ++q)
+    if (a.m->dim(o.l_inner[q]) != bp->dim(o.r_inner[q])) throw DimensionMismatchException("inner dimensions differ");
+  for (size_t q = 0; q < o.l_inter.size(); ++q)
+    if (a.m->dim(o.l_inter[q]) != bp->dim(o.r_inter[q]))
+      throw DimensionMismatchException("element-wise dimensions differ");
+  to_lattice(*a.m, o.l_outer, o.l_inner, o.l_inter);
+  to_lattice(*bp, o.r_inner, o.r_outer, o.r_inter);
+  lnt_lattice A{a.m->keys(), a.m->vals(), a.m->size(), (int64_t)prod_dims(*a.m, o.l_outer),
+                (int64_t)prod_dims(*a.m, o.l_inner), (int64_t)prod_dims(*a.m, o.l_inter)};
+  lnt_lattice B{bp->keys(), bp->vals(), bp->size(), (int64_t)prod_dims(*bp, o.r_inner),
+                (int64_t)prod_dims(*bp, o.r_outer), (int64_t)prod_dims(*bp, o.r_inter)};
+  size_t plan_bytes = 0;
+  check(lnt_lattice_mult_plan_workspace(&A, &B, &plan_bytes), "product");
+  DeviceBuffer<unsigned char> plan(plan_bytes);
+  DeviceBuffer<uint64_t> counts(2);
+  check(lnt_lattice_mult_plan(&A, &B, plan.data(), plan_bytes, counts.data(), nullptr), "product");
+  uint64_t hc[2];
+  cuda_check(cudaMemcpy(hc, counts.data(), 16, cudaMemcpyDeviceToHost), "product counts");
+  size_t need = 0;
+  check(lnt_lattice_mult_workspace(&A, &B, hc[0], &need), "product");
+  DeviceBuffer<uint64_t> k(std::max<uint64_t>(hc[1], 1));
+  DeviceBuffer<double> v(std::max<uint64_t>(hc[1], 1));
+  DeviceBuffer<uint64_t> nc(1);
+  check(lnt_lattice_mult(&A, &B, plan.data(), hc[0], scratch(need), need, k.data(), v.data(), nc.data(), nullptr),
+        "product");
+  const uint64_t m = read_u64(nc.data());
+  k.shrink(m);
+  v.shrink(m);
+  std::vector<int64_t> dims;
+  Labels labels;
+  for (int i : o.l_outer) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  for (int j : o.r_outer) dims.push_back(bp->dim(j)), labels.push_back(b.labels[j]);
+  for (int i : o.l_inter) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  SparseTensor c(dims);  // default sequence, sorted (SparseMIA.h:362-372)
+  c.take(std::move(k), std::move(v));
+  c.setSorted(true);
+  return {std::move(c), std::move(labels)};
+}
+
+}  // namespace detail
+
+inline SparseExpr operator+(SparseAtom a, SparseAtom b) { return detail::merge(a, b, 0); }
+inline SparseExpr operator-(SparseAtom a, SparseAtom b) { return detail::merge(a, b, 1); }
+inline SparseExpr operator*(SparseAtom a, SparseAtom b) { return detail::product(a, b); }
+
+// Destructive merges (perform_destructive_merge -> SparseMIA::merge, SparseMIA.h:1030-1060):
+// the result replaces the left operand.
+inline SparseAtom& SparseAtom::operator+=(const SparseAtom& o) {
+  SparseAtom b = o;
+  SparseExpr e = detail::merge(*this, b, 0);
+  *m = std::move(e.t);
+  return *this;
+}
+inline SparseAtom& SparseAtom::operator-=(const SparseAtom& o) {
+  SparseAtom b = o;
+  SparseExpr e = detail::merge(*this, b, 1);
+  *m = std::move(e.t);
+  return *this;
+}
+
+// SparseNT<N> / SparseMIA<double, N>: a SparseTensor of fixed order N.
+template <size_t N>
+class SparseNT : public SparseTensor {
+ public:
+  SparseNT() : SparseTensor(std::vector<int64_t>(N, 1)) {}
+  template <class... D, typename = std::enable_if_t<sizeof...(D) == N>>
+  explicit SparseNT(D... dims) : SparseTensor(std::vector<int64_t>{(int64_t)dims...}) {}
+  template <class... I, typename = std::enable_if_t<sizeof...(I) == N>>
+  SparseAtom operator()(const I&... idx) {
+    return SparseAtom{this, Labels{idx...}};
+  }
+  SparseNT& operator=(SparseTensor&& t) {
+    if (t.order() != N) throw MIAParameterException("order mismatch");
+    SparseTensor::operator=(std::move(t));
+    return *this;
+  }
+};
+template <class T, size_t N>
+using SparseMIA = SparseNT<N>;
+
+// ---- dense tensors -------------------------------------------------------------
+// Column-major dense multi-index array (DenseMIA<double, N>); products run as
+// lattice products (DenseLatticeBase::operator*), in float64 or split
+// precision (INT8 tensor-core slices, error about 2^(1-7s) |A||B|).
+class DenseTensor {
+ public:
+  DenseTensor() = default;
+  explicit DenseTensor(std::vector<int64_t> dims) : dims_(std::move(dims)) { data_.resize(numel()); }
+  size_t order() const { return dims_.size(); }
+  const std::vector<int64_t>& dims() const { return dims_; }
+  int64_t dim(size_t i) const { return dims_[i]; }
+  size_t numel() const {
+    size_t n = 1;
+    for (auto d : dims_) n *= (size_t)d;
+    return n;
+  }
+  double* data() { return data_.data(); }
+  const double* data() const { return data_.data(); }
+  void upload(const std::vector<double>& h) {
+    if (h.size() != numel()) throw MIAParameterException("size mismatch");
+    cuda_check(cudaMemcpy(data(), h.data(), h.size() * 8, cudaMemcpyHostToDevice), "upload");
+  }
+  void download(std::vector<double>& h) const {
+    h.resize(numel());
+    cuda_check(cudaMemcpy(h.data(), data(), h.size() * 8, cudaMemcpyDeviceToHost), "download");
+  }
+  static int& slices() {  // 0: plain float64 products; 5..8: split precision
+    thread_local int s = 0;
+    return s;
+  }
+
+ private:
+  std::vector<int64_t> dims_;
+  DeviceBuffer<double> data_;
+};
+
+struct DenseExpr {
+  DenseTensor t;
+  Labels labels;
+};
+
+struct DenseAtom {
+  DenseTensor* m;
+  Labels labels;
+  DenseAtom& operator=(DenseExpr&& e) {
+    if (e.labels != labels)
+      throw MIAParameterException("dense assignment with a different label order is not on this path");
+    *m = std::move(e.t);
+    return *this;
+  }
+};
+
+inline DenseExpr operator*(DenseAtom a, DenseAtom b) {
+  const detail::ProductOrders o = detail::product_orders(a.labels, b.labels);
+  auto consecutive = [](const std::vector<int>& x, const std::vector<int>& y, const std::vector<int>& z) {
+    std::vector<int> s = x;
+    s.insert(s.end(), y.begin(), y.end());
+    s.insert(s.end(), z.begin(), z.end());
+    for (size_t i = 0; i < s.size(); ++i)
+      if (s[i] != (int)i) return false;
+    return true;
+  };
+  // zero-copy lattices (DenseMIA::toStraightLattice, DenseMIA.h:1240-1255); permuted
+  // copies (latticeCopy) are not on this path
+  if (!consecutive(o.l_outer, o.l_inner, o.l_inter) || !consecutive(o.r_inner, o.r_outer, o.r_inter))
+    throw MIAParameterException("dense product needs modes already in lattice order");
+  auto pd = [](const DenseTensor& t, const std::vector<int>& m) {
+    int64_t p = 1;
+    for (int i : m) p *= t.dim(i);
+    return p;
+  };
+  const int64_t h = pd(*a.m, o.l_outer), w = pd(*a.m, o.l_inner), d = pd(*a.m, o.l_inter);
+  const int64_t wB = pd(*b.m, o.r_outer);
+  if (pd(*b.m, o.r_inner) != w || pd(*b.m, o.r_inter) != d) throw DimensionMismatchException("dense product dims");
+  std::vector<int64_t> dims;
+  Labels labels;
+  for (int i : o.l_outer) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  for (int j : o.r_outer) dims.push_back(b.m->dim(j)), labels.push_back(b.labels[j]);
+  for (int i : o.l_inter) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  DenseTensor c(dims);
+  const int s = DenseTensor::slices();
+  if (s == 0) {
+    size_t need = 0;
+    check(lnt_dense_fp64_workspace(&need), "dense product");
+    check(lnt_dense_lattice_mult_fp64(a.m->data(), b.m->data(), c.data(), h, w, wB, d, scratch(need), need,
+                                      nullptr),
+          "dense product");
+  } else {
+    size_t need = 0;
+    check(lnt_dense_split_workspace(h, w, wB, s, &need), "dense product");
+    check(lnt_dense_lattice_mult_split(a.m->data(), b.m->data(), c.data(), h, w, wB, d, s, scratch(need), need,
+                                       nullptr),
+          "dense product");
+  }
+  return {std::move(c), std::move(labels)};
+}
+
+template <size_t N>
+class DenseNT : public DenseTensor {
+ public:
+  template <class... D, typename = std::enable_if_t<sizeof...(D) == N>>
+  explicit DenseNT(D... dims) : DenseTensor(std::vector<int64_t>{(int64_t)dims...}) {}
+  template <class... I, typename = std::enable_if_t<sizeof...(I) == N>>
+  DenseAtom operator()(const I&... idx) {
+    return DenseAtom{this, Labels{idx...}};
+  }
+};
+template <class T, size_t N>
+using DenseMIA = DenseNT<N>;
+
+}  // namespace lnt

@@ -1,0 +1,161 @@
+"""GPU: the C++ index-label front end (lnt::SparseNT / DenseNT with lnt::Index
+labels) against the oracle's restatement of the reference's expression layer,
+including the side effects on the operands (linIdxSequence, sorted flag,
+re-keyed / re-sorted storage)."""
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from frontend_build import build
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def driver(cuda):
+    return build()
+
+
+def write(d, name, m):
+    (d / f"{name}.keys").write_bytes(np.ascontiguousarray(m.keys, np.uint64).tobytes())
+    (d / f"{name}.vals").write_bytes(np.ascontiguousarray(m.vals, np.float64).tobytes())
+    (d / f"{name}.meta").write_text(f"{m.order} {' '.join(map(str, m.dims))} {' '.join(map(str, m.seq))} "
+                                    f"{int(m.sorted)}\n")
+
+
+def read(d, name):
+    meta = (d / f"{name}.meta").read_text().split()
+    order = int(meta[0])
+    dims = [int(x) for x in meta[1:1 + order]]
+    seq = [int(x) for x in meta[1 + order:1 + 2 * order]]
+    return oracle.SparseMIA(dims, np.frombuffer((d / f"{name}.keys").read_bytes(), np.uint64),
+                            np.frombuffer((d / f"{name}.vals").read_bytes(), np.float64), seq,
+                            bool(int(meta[1 + 2 * order])))
+
+
+def run(driver, scenario, d):
+    r = subprocess.run([str(driver), scenario, str(d)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+
+
+def same(got, exp, atol=1e-12):
+    assert got.dims == exp.dims and got.seq == exp.seq and got.sorted == exp.sorted, \
+        (got.dims, exp.dims, got.seq, exp.seq, got.sorted, exp.sorted)
+    np.testing.assert_array_equal(got.keys, exp.keys)
+    np.testing.assert_allclose(got.vals, exp.vals, rtol=0, atol=atol)
+
+
+def rand_mia(rng, dims, n, sorted_=False, seq=None, unique=True):
+    total = int(np.prod(dims))
+    keys = (rng.choice(total, n, replace=False) if unique else rng.integers(0, total, n)).astype(np.uint64)
+    m = oracle.SparseMIA(dims, keys, rng.uniform(-1, 1, n), sorted=False)
+    if seq is not None:
+        m.change_linIdx_sequence(seq)
+    if sorted_:
+        m.sort()
+    return m
+
+
+@pytest.mark.parametrize("scenario", ["product", "product_assign"])
+@pytest.mark.parametrize("n", [2000, 10000])
+def test_product(driver, tmp_path, rng, scenario, n):
+    """c(i,l) = a(i,j,k) * b(k,l,j) (and c(l,i) = ...): toStraightLattice /
+    toLatticeSort side effects on a and b, sorted default-sequence result."""
+    a = rand_mia(rng, [100, 30, 40], n)
+    b = rand_mia(rng, [40, 50, 30], n, sorted_=(n == 2000))
+    write(tmp_path, "a", a)
+    write(tmp_path, "b", b)
+    run(driver, scenario, tmp_path)
+    ea, eb = a.copy(), b.copy()
+    c, lab = oracle.product(ea, list("ijk"), eb, list("klj"))
+    if scenario == "product_assign":
+        c = oracle.assign(list("li"), c, lab)
+    same(read(tmp_path, "c"), c)
+    same(read(tmp_path, "a_after"), ea, atol=0)
+    same(read(tmp_path, "b_after"), eb, atol=0)
+
+
+def test_elementwise_product(driver, tmp_path, rng):
+    a = rand_mia(rng, [30, 20, 6], 800)
+    b = rand_mia(rng, [20, 25, 6], 800)
+    write(tmp_path, "a", a)
+    write(tmp_path, "b", b)
+    run(driver, "elementwise", tmp_path)
+    c, _ = oracle.product(a.copy(), ["i", "j", "!n"], b.copy(), ["j", "l", "!n"])
+    same(read(tmp_path, "c"), c)
+
+
+@pytest.mark.parametrize("a_state,b_state", [("unsorted", "unsorted"), ("sorted", "unsorted"),
+                                             ("unsorted", "sorted"), ("sorted", "sorted"),
+                                             ("sorted_other", "unsorted"), ("unsorted", "sorted_other")])
+@pytest.mark.parametrize("na,nb", [(5000, 5000), (6000, 4000), (2000, 2500)])
+@pytest.mark.parametrize("scenario", ["merge_add", "merge_sub"])
+def test_merge_branches(driver, tmp_path, rng, a_state, b_state, na, nb, scenario):
+    """c(i,j,k,l) = a(i,j,k,l) +/- b(l,k,j,i) through every branch of
+    perform_outside_merge, with the operands' post-states."""
+    dims = [12, 10, 14, 9]
+    a = rand_mia(rng, dims, na, unique=False)
+    b = rand_mia(rng, dims[::-1], nb, unique=False)
+    for m, st in ((a, a_state), (b, b_state)):
+        if st == "sorted":
+            m.collect_duplicates()
+        elif st == "sorted_other":
+            m.collect_duplicates()
+            m.sort([1, 3, 0, 2])
+    write(tmp_path, "a", a)
+    write(tmp_path, "b", b)
+    run(driver, scenario, tmp_path)
+    ea, eb = a.copy(), b.copy()
+    c = oracle.merge(ea, eb, [3, 2, 1, 0], 0 if scenario == "merge_add" else 1)
+    same(read(tmp_path, "c"), c)
+    same(read(tmp_path, "a_after"), ea, atol=0)
+    same(read(tmp_path, "b_after"), eb, atol=0)
+
+
+def test_self_merge_and_plus_equals(driver, tmp_path, rng):
+    dims = [8, 8, 8, 8]
+    a = rand_mia(rng, dims, 1500)
+    b = rand_mia(rng, dims, 1500)
+    write(tmp_path, "a", a)
+    write(tmp_path, "b", b)
+    run(driver, "merge_self", tmp_path)
+    c = oracle.merge(a.copy(), a.copy(), [3, 2, 1, 0])
+    same(read(tmp_path, "c"), c)
+    run(driver, "plus_equals", tmp_path)
+    c = oracle.merge(a.copy(), b.copy(), [3, 2, 1, 0])
+    same(read(tmp_path, "c"), c)
+
+
+@pytest.mark.parametrize("n,sorted_", [(2000, True), (5000, True), (5000, False)])
+def test_sort_seq_and_collect(driver, tmp_path, rng, n, sorted_):
+    dims = [9, 11, 7, 13]
+    a = rand_mia(rng, dims, n, sorted_=sorted_)
+    write(tmp_path, "a", a)
+    run(driver, "sort_seq", tmp_path)
+    e = a.copy()
+    e.sort([2, 0, 3, 1])  # incl. the < 3000 branch that leaves the flag cleared
+    same(read(tmp_path, "c"), e, atol=0)
+    a2 = rand_mia(rng, dims, n, unique=False)
+    a2.vals[rng.random(n) < 0.3] = 0.0
+    write(tmp_path, "a", a2)
+    run(driver, "collect", tmp_path)
+    e2 = a2.copy()
+    e2.collect_duplicates()
+    same(read(tmp_path, "c"), e2)
+
+
+@pytest.mark.parametrize("slices", [0, 7])
+def test_dense_product(driver, tmp_path, rng, slices):
+    """c(i,j,m,n) = a(i,j,k,l) * b(k,l,m,n) on DenseNT<4>, float64 and split."""
+    d1, d2 = 6, 5
+    A = rng.uniform(-1, 1, d1 * d1 * d2 * d2)
+    B = rng.uniform(-1, 1, d2 * d2 * d1 * d1)
+    (tmp_path / "A.vals").write_bytes(A.tobytes())
+    (tmp_path / "B.vals").write_bytes(B.tobytes())
+    (tmp_path / "dense.meta").write_text(f"{d1} {d2} {slices}\n")
+    run(driver, "dense", tmp_path)
+    got = np.frombuffer((tmp_path / "C.vals").read_bytes(), np.float64)
+    ref = oracle.dense_lattice_mult(A, B, d1 * d1, d2 * d2, d1 * d1, 1)
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-13)
