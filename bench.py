@@ -578,7 +578,9 @@ def run_batched(args):
 
 
 def run_dense(args):
-    """c(i,j,m,n) = a(i,j,k,l) * b(k,l,m,n), all dims 128: a 16384^3 FP64 GEMM."""
+    """c(i,j,m,n) = a(i,j,k,l) * b(k,l,m,n), all dims 128: a 16384^3 FP64 GEMM.
+    Headline: scheme II (moduli + Chinese remaindering) on INT8 tensor cores;
+    also timed: scheme I (INT8 slices) and the plain FP64 GEMM."""
     import torch
 
     import libnt_b200 as L
@@ -589,7 +591,26 @@ def run_dense(args):
     g = torch.Generator(device=dev)
     g.manual_seed(5 + rank)
     results = {}
+    flops = 2.0 * n ** 3
+    reps = max(1, min(args.steps, 5))
+
+    def timed(fn):
+        for _ in range(max(1, args.warmup // 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    rows = np.random.default_rng(1).integers(0, n, 1024)
+    cols = np.random.default_rng(2).integers(0, n, 1024)
+    idx = rows + n * cols
     for variant in ("uniform", "wide_exponent"):
+        moduli = args.moduli if variant == "uniform" else max(args.moduli, 16)
         slices = args.slices if variant == "uniform" else max(args.slices, 8)
         if variant == "uniform":
             A = torch.rand(n * n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
@@ -601,61 +622,49 @@ def run_dense(args):
                 sgn = torch.randint(0, 2, (n * n,), generator=g, device=dev).to(torch.float64) * 2 - 1
                 return m * torch.pow(2.0, e) * sgn
             A, B = wide(), wide()
-        ws = L.workspace(L.dense_split_workspace(n, n, n, slices), dev)
-        ws64 = L.workspace(64 << 20, dev)
-        Cs = torch.empty(n * n, dtype=torch.float64, device=dev)
+        Cc = torch.empty(n * n, dtype=torch.float64, device=dev)
         C64 = torch.empty(n * n, dtype=torch.float64, device=dev)
-        for _ in range(max(1, args.warmup // 3)):
-            L.dense_mult_split(A, B, n, n, n, 1, slices, out=Cs, ws=ws)
-            L.dense_mult_fp64(A, B, n, n, n, 1, out=C64, ws=ws64)
-        torch.cuda.synchronize()
-        reps = max(1, min(args.steps, 5))
+        ws64 = L.workspace(64 << 20, dev)
+        t64 = timed(lambda: L.dense_mult_fp64(A, B, n, n, n, 1, out=C64, ws=ws64))
+        wsc = L.workspace(L.dense_crt_workspace(n, n, n, moduli), dev)
         L.profile_reset()
         L.profile_enable(True)
-        e0, e1 = _events()
         sampler = ClockSampler(torch.cuda.current_device())
         with sampler:
-            e0.record()
-            for _ in range(reps):
-                L.dense_mult_split(A, B, n, n, n, 1, slices, out=Cs, ws=ws)
-            e1.record()
-            torch.cuda.synchronize()
+            t_crt = timed(lambda: L.dense_mult_crt(A, B, n, n, n, 1, moduli, out=Cc, ws=wsc))
         L.profile_enable(False)
-        t_split = e0.elapsed_time(e1) / reps
-        kern = {k: L.profile_query(k) for k in ("dense_split", "dense_int8_gemm", "dense_recombine")}
+        kern = {k: L.profile_query(k)[0] / (reps + max(1, args.warmup // 3))
+                for k in ("dense_residues", "dense_int8_gemm", "dense_crt")}
         L.profile_reset()
-        f0, f1 = _events()
-        f0.record()
-        for _ in range(reps):
-            L.dense_mult_fp64(A, B, n, n, n, 1, out=C64, ws=ws64)
-        f1.record()
-        torch.cuda.synchronize()
-        t64 = f0.elapsed_time(f1) / reps
-        # error: sampled entries against compensated FP64 dots on the host
-        ns = 1024
-        rows = np.random.default_rng(1).integers(0, n, ns)
-        cols = np.random.default_rng(2).integers(0, n, ns)
-        Ah = A.cpu().numpy()
-        Bh = B.cpu().numpy()
+        del wsc
+        torch.cuda.empty_cache()
+        Ah, Bh = A.cpu().numpy(), B.cpu().numpy()
         ref, mag = oracle.dense_entries(Ah, Bh, n, n, rows, cols)
-        Csh = Cs.cpu().numpy()
-        C64h = C64.cpu().numpy()
-        idx = rows + n * cols
-        err_ab = float(np.max(np.abs(Csh[idx] - ref) / mag))
-        err_rel = float(np.max(np.abs(Csh[idx] - ref) / np.maximum(np.abs(ref), 1e-300)))
-        err64_ab = float(np.max(np.abs(C64h[idx] - ref) / mag))
-        full = float((Cs - C64).abs().max().item() / C64.abs().max().item())
-        flops = 2.0 * n ** 3
-        gemm_ms = kern["dense_int8_gemm"][0] / reps
-        int8_ops = sum((L_ + 1) for L_ in range(slices)) * 2.0 * n ** 3
-        results[variant] = {"slices": slices, "split_ms": t_split, "fp64_ms": t64, "speedup_vs_fp64": t64 / t_split,
-                            "effective_fp64_tflops": flops / (t_split * 1e-3) / 1e12,
-                            "fp64_tflops": flops / (t64 * 1e-3) / 1e12,
-                            "max_err_rel_absAabsB": err_ab, "max_err_rel_C": err_rel, "fp64_err_rel_absAabsB": err64_ab,
-                            "max_diff_vs_fp64_over_maxC": full, "sampled_entries": ns,
-                            "kernels_ms_per_step": {k: v[0] / reps for k, v in kern.items()},
-                            "int8_tensor_tops": int8_ops / (gemm_ms * 1e-3) / 1e12, "clocks": sampler.summary()}
-        del A, B, Cs, C64, ws
+
+        def errors(Cd):
+            Ch = Cd.cpu().numpy()[idx]
+            return (float(np.max(np.abs(Ch - ref) / mag)),
+                    float(np.max(np.abs(Ch - ref) / np.maximum(np.abs(ref), 1e-300))))
+        e_crt = errors(Cc)
+        e_64 = errors(C64)
+        full = float((Cc - C64).abs().max().item() / C64.abs().max().item())
+        res = {"moduli": moduli, "crt_ms": t_crt, "fp64_ms": t64, "speedup_vs_fp64": t64 / t_crt,
+               "effective_fp64_tflops": flops / (t_crt * 1e-3) / 1e12, "fp64_tflops": flops / (t64 * 1e-3) / 1e12,
+               "max_err_rel_absAabsB": e_crt[0], "max_err_rel_C": e_crt[1],
+               "fp64_gemm_err_rel_absAabsB": e_64[0], "fp64_gemm_err_rel_C": e_64[1],
+               "max_diff_vs_fp64_over_maxC": full, "sampled_entries": int(rows.size),
+               "kernels_ms_per_step": kern,
+               "int8_tensor_tops": moduli * 2.0 * n ** 3 / (kern["dense_int8_gemm"] * 1e-3) / 1e12,
+               "clocks": sampler.summary()}
+        if not args.no_scheme1:
+            wss = L.workspace(L.dense_split_workspace(n, n, n, slices), dev)
+            t_split = timed(lambda: L.dense_mult_split(A, B, n, n, n, 1, slices, out=Cc, ws=wss))
+            es = errors(Cc)
+            res["scheme1_slices"] = {"slices": slices, "ms": t_split, "speedup_vs_fp64": t64 / t_split,
+                                     "max_err_rel_absAabsB": es[0]}
+            del wss
+        results[variant] = res
+        del A, B, Cc, C64
         torch.cuda.empty_cache()
     if rank != 0:
         return 0
@@ -673,18 +682,18 @@ def run_dense(args):
     torch.cuda.synchronize()
     int8_peak = 2 * 8192 ** 3 / (e0.elapsed_time(e1) / 10 * 1e-3) / 1e12
     u = results["uniform"]
-    config = {"workload": f"dense contraction c(i,j,m,n)=a(i,j,k,l)*b(k,l,m,n), dims 128 (a {n}^3 FP64 GEMM), "
-                          f"split into INT8 slices (7 for U[-1,1], 8 for 2^+-20 exponents), INT32 tensor products, "
-                          f"FP64 recombination",
+    config = {"workload": f"dense contraction c(i,j,m,n)=a(i,j,k,l)*b(k,l,m,n), dims 128 (a {n}^3 FP64 GEMM); "
+                          "Ozaki scheme II: beta-bit integer operands, 13 (U[-1,1]) / 16 (2^+-20 exponents) moduli "
+                          "<= 256 as INT8 tensor-core GEMMs, Chinese remaindering in double-double",
               "variants": results}
-    print(json.dumps(_line("TFLOP/s (FP64-equivalent)", u["effective_fp64_tflops"], u["split_ms"], args, world, config, {
-        "roofline": {"bound": "tensor", "kernel": "INT8 level GEMMs", "achieved": u["int8_tensor_tops"],
+    print(json.dumps(_line("TFLOP/s (FP64-equivalent)", u["effective_fp64_tflops"], u["crt_ms"], args, world,
+                           config, {
+        "roofline": {"bound": "tensor", "kernel": "INT8 modular GEMMs", "achieved": u["int8_tensor_tops"],
                      "peak": int8_peak, "unit": "TOP/s", "frac": u["int8_tensor_tops"] / int8_peak,
                      "peak_source": "int8 torch._int_mm 8192^3 measured in this run (MEASURED_PEAKS.json has bf16 only)"},
         "vs_fp64_gemm": u["speedup_vs_fp64"], "clocks": u["clocks"],
     })), flush=True)
     return 0
-
 
 def main():
     ap = argparse.ArgumentParser()
@@ -699,7 +708,9 @@ def main():
     ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense"],
                     help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
                          "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")
-    ap.add_argument("--slices", type=int, default=7, help="dense: INT8 slices per operand")
+    ap.add_argument("--slices", type=int, default=7, help="dense scheme I: INT8 slices per operand")
+    ap.add_argument("--moduli", type=int, default=13, help="dense scheme II: moduli (uniform data)")
+    ap.add_argument("--no-scheme1", action="store_true", help="dense: skip timing scheme I")
     ap.add_argument("--dense-log2", type=int, default=14, help="dense: log2 of the GEMM size (14 = the workload)")
     args = ap.parse_args()
     if args.warmup < 3:

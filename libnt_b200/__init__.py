@@ -98,6 +98,9 @@ _SIGS = {
     "lnt_dense_split_workspace": ([C.c_int64, C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_size_t)], C.c_int),
     "lnt_dense_lattice_mult_split": ([_vp, _vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, _vp,
                                       _sz, _vp], C.c_int),
+    "lnt_dense_crt_workspace": ([C.c_int64, C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_dense_lattice_mult_crt": ([_vp, _vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, _vp,
+                                    _sz, _vp], C.c_int),
 }
 
 _lib = None
@@ -413,4 +416,22 @@ def dense_mult_fp64(A, B, h: int, w: int, wB: int, d: int = 1, out=None, ws=None
         ws = workspace(64 << 20, A.device)
     _check(lib().lnt_dense_lattice_mult_fp64(_ptr(A), _ptr(B), _ptr(Cm), h, w, wB, d, _ptr(ws), ws.numel(),
                                              _stream()), "lnt_dense_lattice_mult_fp64")
+    return Cm
+
+
+def dense_crt_workspace(h: int, w: int, wB: int, moduli: int = 13) -> int:
+    b = C.c_size_t(0)
+    _check(lib().lnt_dense_crt_workspace(h, w, wB, moduli, C.byref(b)), "lnt_dense_crt_workspace")
+    return b.value
+
+
+def dense_mult_crt(A, B, h: int, w: int, wB: int, d: int = 1, moduli: int = 13, out=None, ws=None):
+    """Dense lattice product by integer moduli + Chinese remaindering (scheme II)."""
+    torch = _torch()
+    Cm = torch.empty(h * wB * d, dtype=torch.float64, device=A.device) if out is None else out
+    need = dense_crt_workspace(h, w, wB, moduli)
+    if ws is None or ws.numel() < need:
+        ws = workspace(need, A.device)
+    _check(lib().lnt_dense_lattice_mult_crt(_ptr(A), _ptr(B), _ptr(Cm), h, w, wB, d, moduli, _ptr(ws), ws.numel(),
+                                            _stream()), "lnt_dense_lattice_mult_crt")
     return Cm

@@ -259,6 +259,251 @@ int lt_dgemm(const double* A, const double* B, double* C, u64 m, u64 n, u64 k, v
   return st;
 }
 
+
+// ===========================================================================
+// Scheme II: integer moduli and Chinese remaindering (Ozaki, Uchino, Imamura,
+// "Ozaki Scheme II: A GEMM-oriented emulation of floating-point matrix
+// multiplication using an integer modular technique", 2024).
+//   1. rows of A / columns of B are scaled by powers of two and rounded to
+//      integers A', B' of at most beta bits (|A'| <= 2^(beta-1));
+//   2. for each modulus m_l (pairwise coprime, <= 256) the symmetric residues
+//      A' mod m_l, B' mod m_l fit INT8 and P_l = (A' mod m_l)(B' mod m_l) is an
+//      exact INT8 tensor-core GEMM with INT32 accumulation (|P_l| <= 2^14 K);
+//   3. per entry, y_l = (P_l mod m_l) * ((M/m_l)^-1 mod m_l) mod m_l and
+//      S = sum_l y_l / m_l in double-double; A'B' = M (S - round(S)) exactly as
+//      long as |A'B'| < M/2 (M = prod m_l), which fixes beta:
+//      2 beta <= log2 M - log2 K - 3.
+// The error is the rounding of A and B to beta bits: about 2^(2-beta) |A||B|
+// componentwise; N moduli give beta = floor((log2 M - log2 K - 3) / 2).
+// ===========================================================================
+constexpr int kMaxModuli = 20;
+// pairwise coprime, all <= 256 so symmetric residues fit in int8
+constexpr int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                     223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+
+struct CrtParams {
+  int n;        // moduli used
+  int beta;     // integer bits of A' and B'
+  int m[kMaxModuli];
+  int u[kMaxModuli];            // (M/m_l)^-1 mod m_l
+  double rinv_hi[kMaxModuli];   // 1/m_l as a double-double
+  double rinv_lo[kMaxModuli];
+  float rinv_f[kMaxModuli];     // 1/m_l in float
+  double M_hi, M_lo;            // M as a double-double
+};
+
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// x mod m in [0, m) for an integer-valued double |x| < 2^56 and m <= 256:
+// q = floor(x / m) is off by at most one, and fma(-q, m, x) is exact because
+// the true remainder is a small integer.
+__device__ __forceinline__ double dmod(double x, double m, double inv_m) {
+  const double q = floor(x * inv_m);
+  double r = fma(-q, m, x);
+  if (r < 0.0) r += m;
+  else if (r >= m) r -= m;
+  return r;
+}
+
+// Same for an integer-valued float below 2^24.
+__device__ __forceinline__ float fmod_small(float x, float m, float inv_m) {
+  const float q = floorf(x * inv_m);
+  float r = fmaf(-q, m, x);
+  if (r < 0.f) r += m;
+  else if (r >= m) r -= m;
+  return r;
+}
+
+// 2^e as a double, exact for normal exponents (bit pattern built directly).
+__device__ __forceinline__ double pow2(int e) {
+  if (e >= -1022 && e <= 1023) return __longlong_as_double((long long)(1023 + e) << 52);
+  return ldexp(1.0, e);
+}
+
+// x * 2^e, exact (two factors keep intermediate values normal).
+__device__ __forceinline__ double scale2(double x, int e) {
+  const int e1 = e / 2;
+  return (x * pow2(e1)) * pow2(e - e1);
+}
+
+__device__ __forceinline__ signed char sym_res(double x, int l, const CrtParams& P) {
+  const double m = (double)P.m[l];
+  double r = dmod(x, m, P.rinv_hi[l]);
+  if (r >= (double)((P.m[l] + 1) / 2)) r -= m;
+  return (signed char)(int)r;
+}
+
+// Per-row maximum exponent of A (col-major) over a chunk of columns; eA must
+// start below every double exponent (-4096; an all-zero row keeps it).  e = E + 1 for the row maximum f 2^E, f in [1/2, 1).
+__global__ void row_exp_chunk_kernel(const double* __restrict__ A, u64 h, u64 w, u64 kchunk,
+                                     int* __restrict__ eA) {
+  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= h) return;
+  const u64 k0 = (u64)blockIdx.y * kchunk, k1 = min(w, k0 + kchunk);
+  double m = 0.0;
+  for (u64 k = k0; k < k1; ++k) m = fmax(m, fabs(A[i + h * k]));
+  if (m > 0.0) {
+    int e;
+    frexp(m, &e);
+    atomicMax(&eA[i], e + 1);
+  }
+}
+
+__global__ void fill_int_kernel(int* __restrict__ p, u64 n, int v) {
+  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// A (h x w col-major) -> residues res[l]: Mp rows of Kp int8 (row-major, K
+// contiguous).  Tile of 32 rows x 128 columns through shared memory: read
+// along rows (coalesced), write along K (each warp stores 32 consecutive bytes).
+__global__ void __launch_bounds__(256) residue_a_kernel(const double* __restrict__ A, u64 h, u64 w, u64 Mp, u64 Kp,
+                                                        const int* __restrict__ eA, CrtParams P,
+                                                        signed char* __restrict__ res) {
+  __shared__ double tile[32][129];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const u64 i0 = (u64)blockIdx.x * 32, k0 = (u64)blockIdx.y * 128;
+  for (int kk = warp; kk < 128; kk += 8) {
+    const u64 i = i0 + lane, k = k0 + kk;
+    tile[lane][kk] = (i < h && k < w) ? A[i + h * k] : 0.0;
+  }
+  __syncthreads();
+  for (int rr = warp; rr < 32; rr += 8) {
+    const u64 i = i0 + rr;
+    if (i >= h) continue;
+    const int sc = P.beta - eA[i];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const u64 k = k0 + q * 32 + lane;
+      if (k >= Kp) continue;
+      const double x = rint(scale2(tile[rr][q * 32 + lane], sc));
+      signed char* dst = res + i * Kp + k;
+      for (int l = 0; l < P.n; ++l) dst[(u64)l * Mp * Kp] = sym_res(x, l, P);
+    }
+  }
+}
+
+// B (w x wB col-major) -> residues res[l]: Np rows (columns of B) of Kp int8.
+__global__ void residue_b_kernel(const double* __restrict__ B, u64 w, u64 wB, u64 Np, u64 Kp,
+                                 const int* __restrict__ eB, CrtParams P, signed char* __restrict__ res) {
+  const u64 total = w * wB;
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const u64 j = t / w, k = t - j * w;
+    const double x = rint(scale2(B[t], P.beta - eB[j]));
+    signed char* dst = res + j * Kp + k;
+    for (int l = 0; l < P.n; ++l) dst[(u64)l * Np * Kp] = sym_res(x, l, P);
+  }
+}
+
+// Chinese remaindering of the P.n INT32 products, scaled back to float64.
+// Grid: x over rows of C (coalesced), y over columns.
+__global__ void crt_kernel(const int* __restrict__ prod, u64 Mp, u64 Np, u64 h, u64 wB, CrtParams P,
+                           const int* __restrict__ eA, const int* __restrict__ eB, double* __restrict__ C) {
+  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= h) return;
+  const u64 plane = Mp * Np;
+  const int ea = eA[i] - 2 * P.beta;
+  for (u64 j = blockIdx.y; j < wB; j += gridDim.y) {
+    const u64 src = i + Mp * j;
+    double sh = 0.0, sl = 0.0;  // S as a double-double
+#pragma unroll 4
+    for (int l = 0; l < P.n; ++l) {
+      const double m = (double)P.m[l];
+      const double r = dmod((double)__ldcs(prod + (u64)l * plane + src), m, P.rinv_hi[l]);
+      const float y = fmod_small((float)r * (float)P.u[l], (float)P.m[l], P.rinv_f[l]);
+      const double yd = (double)y;
+      const double ph = yd * P.rinv_hi[l];
+      const double pl = fma(yd, P.rinv_hi[l], -ph) + yd * P.rinv_lo[l];  // y/m_l = ph + pl
+      double s, e;
+      two_sum(sh, ph, s, e);
+      e += sl + pl;
+      two_sum(s, e, sh, sl);
+    }
+    const double q = rint(sh);
+    double f, fe;
+    two_sum(sh - q, sl, f, fe);  // S - round(S), |.| < 1/2
+    // A'B' = M (S - q): double-double product, rounded once
+    const double c = f * P.M_hi + (fma(f, P.M_hi, -f * P.M_hi) + fe * P.M_hi + f * P.M_lo);
+    C[i + h * j] = scale2(c, ea + eB[j]);
+  }
+}
+
+struct CrtLayout {
+  u64 Kp, Mp, Np;
+  size_t off_ea, off_eb, off_ra, off_rb, off_prod, off_lt, lt_bytes, total;
+};
+
+CrtLayout crt_layout(u64 h, u64 w, u64 wB, int n) {
+  CrtLayout L;
+  L.Kp = (w + 15) / 16 * 16;
+  L.Mp = (h + 15) / 16 * 16;
+  L.Np = (wB + 15) / 16 * 16;
+  size_t off = 0;
+  L.off_ea = off;
+  off += align_up(h * 4, 256);
+  L.off_eb = off;
+  off += align_up(wB * 4, 256);
+  L.off_ra = off;
+  off += align_up((u64)n * L.Mp * L.Kp, 256);
+  L.off_rb = off;
+  off += align_up((u64)n * L.Np * L.Kp, 256);
+  L.off_prod = off;
+  off += align_up((u64)n * L.Mp * L.Np * 4, 256);
+  L.lt_bytes = 64ull << 20;
+  L.off_lt = off;
+  off += L.lt_bytes;
+  L.total = off;
+  return L;
+}
+
+// Host: moduli tables for n moduli and inner dimension K.
+int make_crt_params(int n, u64 K, CrtParams* P) {
+  if (n < 2 || n > kMaxModuli) return LNT_BAD_ARG;
+  P->n = n;
+  double log2M = 0.0;
+  for (int l = 0; l < n; ++l) {
+    P->m[l] = kModuli[l];
+    log2M += std::log2((double)kModuli[l]);
+  }
+  const int beta = (int)std::floor((log2M - std::log2((double)K) - 3.0) / 2.0);
+  if (beta < 8) return LNT_UNSUPPORTED;
+  P->beta = std::min(beta, 62);
+  for (int l = 0; l < n; ++l) {
+    const int m = P->m[l];
+    long long rest = 1;  // (M / m) mod m
+    for (int q = 0; q < n; ++q)
+      if (q != l) rest = rest * (P->m[q] % m) % m;
+    int inv = 0;  // modular inverse by search (m <= 256)
+    for (int x = 1; x < m; ++x)
+      if (rest * x % m == 1) {
+        inv = x;
+        break;
+      }
+    if (!inv) return LNT_BAD_ARG;
+    P->u[l] = inv;
+    P->rinv_hi[l] = 1.0 / m;
+    P->rinv_lo[l] = std::fma(-P->rinv_hi[l], (double)m, 1.0) / m;
+    P->rinv_f[l] = 1.0f / (float)m;
+  }
+  // M as a double-double (products of small integers, exact residual by fma)
+  double mh = 1.0, ml = 0.0;
+  for (int l = 0; l < n; ++l) {
+    const double m = (double)P->m[l];
+    const double ph = mh * m;
+    const double pl = std::fma(mh, m, -ph) + ml * m;
+    mh = ph + pl;
+    ml = pl - (mh - ph);
+  }
+  P->M_hi = mh;
+  P->M_lo = ml;
+  return LNT_OK;
+}
+
 int check_dense(int64_t h, int64_t w, int64_t wB, int64_t d) {
   if (h <= 0 || w <= 0 || wB <= 0 || d <= 0) return LNT_BAD_DIMS;
   if (h > (1ll << 31) || w > (1ll << 31) || wB > (1ll << 31)) return LNT_UNSUPPORTED;
@@ -329,6 +574,77 @@ int lnt_dense_lattice_mult_split(const double* A, const double* B, double* C, in
     {
       ProfScope prof("dense_recombine", s);
       recombine_kernel<<<sms * 16, 256, 0, s>>>(lev, L.Mp, L.Np, slices, uh, uwB, eA, eB, Ct);
+      count_launch();
+    }
+  }
+  return launch_status();
+}
+
+
+int lnt_dense_crt_workspace(int64_t h, int64_t w, int64_t wB, int moduli, size_t* bytes) {
+  int st = check_dense(h, w, wB, 1);
+  if (st != LNT_OK) return st;
+  if (!bytes) return LNT_BAD_ARG;
+  if ((u64)w >= (1ull << 17)) return LNT_UNSUPPORTED;  // INT32 exactness: K * 2^14 < 2^31
+  CrtParams P;
+  st = make_crt_params(moduli, (u64)w, &P);
+  if (st != LNT_OK) return st;
+  *bytes = crt_layout(h, w, wB, moduli).total;
+  return LNT_OK;
+}
+
+int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int64_t h, int64_t w, int64_t wB,
+                               int64_t d, int moduli, void* workspace, size_t workspace_bytes, void* stream) {
+  int st = check_dense(h, w, wB, d);
+  if (st != LNT_OK) return st;
+  if (!A || !B || !C) return LNT_BAD_ARG;
+  size_t need = 0;
+  st = lnt_dense_crt_workspace(h, w, wB, moduli, &need);
+  if (st != LNT_OK) return st;
+  if (!workspace || workspace_bytes < need || (uintptr_t)workspace % 256) return LNT_WORKSPACE;
+  CrtParams P;
+  st = make_crt_params(moduli, (u64)w, &P);
+  if (st != LNT_OK) return st;
+  const CrtLayout L = crt_layout(h, w, wB, moduli);
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  int* eA = reinterpret_cast<int*>(ws + L.off_ea);
+  int* eB = reinterpret_cast<int*>(ws + L.off_eb);
+  signed char* ra = reinterpret_cast<signed char*>(ws + L.off_ra);
+  signed char* rb = reinterpret_cast<signed char*>(ws + L.off_rb);
+  int* prod = reinterpret_cast<int*>(ws + L.off_prod);
+  cudaStream_t s = as_stream(stream);
+  const int sms = sm_count();
+  const u64 uh = h, uw = w, uwB = wB, Kp = L.Kp;
+  for (int64_t t = 0; t < d; ++t) {
+    const double* At = A + (u64)t * uh * uw;
+    const double* Bt = B + (u64)t * uw * uwB;
+    double* Ct = C + (u64)t * uh * uwB;
+    {
+      ProfScope prof("dense_residues", s);
+      const u64 kchunk = 256;
+      fill_int_kernel<<<(unsigned)((uh + 255) / 256), 256, 0, s>>>(eA, uh, -4096);  // below any double exponent
+      row_exp_chunk_kernel<<<dim3((unsigned)((uh + 255) / 256), (unsigned)((uw + kchunk - 1) / kchunk)), 256, 0, s>>>(
+          At, uh, uw, kchunk, eA);
+      col_exp_kernel<<<(unsigned)((uwB * 32 + 255) / 256), 256, 0, s>>>(Bt, uw, uwB, eB);
+      if (Kp != uw || L.Mp != uh || L.Np != uwB) {  // zero every padding row and column
+        if (cudaMemsetAsync(ra, 0, (u64)moduli * L.Mp * Kp, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+        if (cudaMemsetAsync(rb, 0, (u64)moduli * L.Np * Kp, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+      }
+      residue_a_kernel<<<dim3((unsigned)((uh + 31) / 32), (unsigned)((Kp + 127) / 128)), 256, 0, s>>>(
+          At, uh, uw, L.Mp, Kp, eA, P, ra);
+      residue_b_kernel<<<sms * 16, 256, 0, s>>>(Bt, uw, uwB, L.Np, Kp, eB, P, rb);
+      count_launch(5);
+    }
+    for (int l = 0; l < moduli; ++l) {
+      st = lt_int8_gemm(ra + (u64)l * L.Mp * Kp, (int)Kp, rb + (u64)l * L.Np * Kp, (int)Kp,
+                        prod + (u64)l * L.Mp * L.Np, L.Mp, L.Np, Kp, ws + L.off_lt, L.lt_bytes, s);
+      if (st != LNT_OK) return st;
+      count_launch();
+    }
+    {
+      ProfScope prof("dense_crt", s);
+      const unsigned gy = (unsigned)std::min<u64>(uwB, std::max<u64>(1, (u64)sms * 32 / ((uh + 255) / 256)));
+      crt_kernel<<<dim3((unsigned)((uh + 255) / 256), gy), 256, 0, s>>>(prod, L.Mp, L.Np, uh, uwB, P, eA, eB, Ct);
       count_launch();
     }
   }

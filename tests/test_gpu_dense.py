@@ -71,3 +71,45 @@ def test_split_error_vs_compensated_fp64(cuda, torch, rng, h, w, wB, d, variant,
         got = Cs[t * h * wB:(t + 1) * h * wB].reshape(wB, h).T.ravel()
         err = np.abs(got - ref) / np.maximum(mag, 1e-300)
         assert err.max() <= TOL[(variant, slices)], err.max()
+
+
+# scheme II (moduli + Chinese remaindering): error about 2^(2-beta) |A||B|
+CRT_TOL = {("uniform", 13): 1e-12, ("uniform", 16): 1e-13, ("wide_exponent", 13): 1e-8,
+           ("wide_exponent", 16): 1e-12}
+
+
+def test_crt_golden_fixture_and_kat(cuda, torch):
+    z = np.load(GOLDEN / "dense_lattice_5x5x10.npz")
+    h, w, wB, d = (int(x) for x in z["shape"])
+    mag = np.abs(oracle.dense_lattice_mult(np.abs(z["A"]), np.abs(z["B"]), h, w, wB, d))
+    c = to_host(cuda.dense_mult_crt(to_dev(z["A"], torch), to_dev(z["B"], torch), h, w, wB, d, moduli=13))
+    assert np.all(np.abs(c - z["C"]) <= 1e-13 * mag)
+    dim1, dim2 = 3, 4
+    hh, ww, wwB = dim1 * dim1, dim2 * dim2, dim1 * dim1
+    A = np.empty((hh, ww))
+    A[:, :] = np.arange(1, ww + 1)[None, :]
+    B = np.ones((ww, wwB))
+    c = to_host(cuda.dense_mult_crt(to_dev(A.ravel(order="F"), torch), to_dev(B.ravel(order="F"), torch), hh, ww,
+                                    wwB, 1, moduli=13))
+    assert np.all(c == ww * (ww + 1) / 2)
+
+
+@pytest.mark.parametrize("h,w,wB,d", [(100, 300, 70, 3), (257, 1000, 129, 1), (64, 4096, 64, 1)])
+@pytest.mark.parametrize("variant", ["uniform", "wide_exponent"])
+@pytest.mark.parametrize("moduli", [13, 16])
+def test_crt_error_vs_compensated_fp64(cuda, torch, rng, h, w, wB, d, variant, moduli):
+    if variant == "uniform":
+        A = rng.uniform(-1, 1, h * w * d)
+        B = rng.uniform(-1, 1, w * wB * d)
+    else:
+        A = rng.uniform(1, 2, h * w * d) * 2.0 ** rng.integers(-20, 21, h * w * d) * rng.choice([-1, 1], h * w * d)
+        B = rng.uniform(1, 2, w * wB * d) * 2.0 ** rng.integers(-20, 21, w * wB * d) * rng.choice([-1, 1], w * wB * d)
+    Cs = to_host(cuda.dense_mult_crt(to_dev(A, torch), to_dev(B, torch), h, w, wB, d, moduli=moduli))
+    for t in range(d):
+        At = A[t * h * w:(t + 1) * h * w]
+        Bt = B[t * w * wB:(t + 1) * w * wB]
+        rows, cols = np.meshgrid(np.arange(h), np.arange(wB), indexing="ij")
+        ref, mag = oracle.dense_entries(At, Bt, h, w, rows.ravel(), cols.ravel())
+        got = Cs[t * h * wB:(t + 1) * h * wB].reshape(wB, h).T.ravel()
+        err = np.abs(got - ref) / np.maximum(mag, 1e-300)
+        assert err.max() <= CRT_TOL[(variant, moduli)], err.max()
