@@ -150,13 +150,20 @@ def barrier(world):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """Largest per-rank value (step time): the job is as slow as its slowest rank."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(units_per_rank: int, world: int, ms_max: float) -> float:
+    """Whole-job throughput of `world` replicas: all ranks' units over the slowest rank's time."""
+    return units_per_rank * world / (ms_max * 1e-3)
 
 
 # ---------------------------------------------------------------------------
@@ -269,7 +276,7 @@ def run_ours(args):
     L.profile_enable(False)
     ms = e0.elapsed_time(e1) / args.steps
     ms = max_over_ranks(ms, world)
-    value = n * world / (ms * 1e-3)
+    value = job_throughput(n, world, ms)
     os_ms, os_launches = L.profile_query("sort_onesweep")
     kernels = {}
     for name in ("sort_hist", "sort_onesweep", "collect_lead", "collect"):
