@@ -12,6 +12,7 @@
 //                   writes (key, sum) pairs contiguously.
 // Traffic: 16 B read per input pair + 16 B written per output pair.
 #include <algorithm>
+#include <cstdlib>
 
 #include "lnt_sort.cuh"
 
@@ -292,7 +293,7 @@ SortReduceLayout sort_reduce_layout(size_t n, u64 max_key) {
   L.plan = make_sort_plan(n, max_key);
   size_t off = 0;
   L.off_ctrl = off;
-  off += align_up(L.plan.ctrl_bytes, 256);
+  off += align_up(std::max(L.plan.ctrl_bytes, bucket_ctrl_bytes(n)), 256);
   L.off_k0 = off;
   off += align_up(n * 8, 256);
   L.off_v0 = off;
@@ -366,6 +367,13 @@ int lnt_sort_reduce(const uint64_t* a_keys, const double* a_vals, size_t na, con
   double* v0 = reinterpret_cast<double*>(w + L.off_v0);
   u64* k1 = reinterpret_cast<u64*>(w + L.off_k1);
   double* v1 = reinterpret_cast<double*>(w + L.off_v1);
+  const int key_bits = key_bits_for(max_key);
+  if (bucket_path_applies(n, key_bits) && !getenv("LNT_NO_BUCKETS")) {
+    bool used = false;
+    st = run_bucketed_sort_reduce(src, (u32)n, key_bits, skip_zero_heads, k0, v0, k1, v1, w + L.off_ctrl,
+                                  (u64*)keys_out, vals_out, (u64*)d_nout, s, &used);
+    if (st != LNT_OK || used) return st;
+  }
   st = run_sort(L.plan, src, k0, v0, k1, v1, w + L.off_ctrl, s);
   if (st != LNT_OK) return st;
   return run_collect(k0, v0, n, skip_zero_heads, (u64*)keys_out, vals_out, (u64*)d_nout, w + L.off_coll, s);

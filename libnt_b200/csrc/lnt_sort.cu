@@ -469,6 +469,23 @@ int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, d
 
 namespace lnt {
 
+int run_onesweep_pass8(const PairSource& src, bool first, u64* out_k, double* out_v, u32 n, u32 shift, u32 mask,
+                       const u32* bstart, u32* status, u32* tile_counter, cudaStream_t s) {
+  using Sh = OnesweepShape<8, 256, 16>;
+  constexpr size_t sh = Sh::smem;
+  auto k_first = onesweep_kernel<8, 256, 16, 16, true>;
+  auto k_next = onesweep_kernel<8, 256, 16, 16, false>;
+  cudaFuncSetAttribute(first ? k_first : k_next, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  const u32 ntiles = (n + Sh::TILE - 1) / Sh::TILE;
+  ProfScope prof("sort_onesweep", s);
+  if (first)
+    k_first<<<ntiles, 256, sh, s>>>(src, out_k, out_v, n, shift, mask, bstart, status, tile_counter);
+  else
+    k_next<<<ntiles, 256, sh, s>>>(src, out_k, out_v, n, shift, mask, bstart, status, tile_counter);
+  count_launch();
+  return launch_status();
+}
+
 int sort_variant_count() { return kNumVariants; }
 const SortVariant& sort_variant(int i) { return kVariants[i]; }
 

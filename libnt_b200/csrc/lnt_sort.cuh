@@ -88,4 +88,20 @@ SortPlan make_sort_plan(size_t n, u64 max_key, int variant = -1);
 int run_sort(const SortPlan& plan, const PairSource& src, u64* buf0_k, double* buf0_v, u64* buf1_k,
              double* buf1_v, void* ctrl, cudaStream_t s);
 
+// One digit pass of the 8-bit, 256-thread, 16-key onesweep kernel with
+// caller-given digit (shift, mask), exclusive bin starts (256 entries) and a
+// zeroed look-back array (kOnesweepPassTile-pair tiles x 256 digits) and tile
+// counter.  Used by the bucketed sort.
+constexpr u32 kOnesweepPassTile = 4096;
+int run_onesweep_pass8(const PairSource& src, bool first, u64* out_k, double* out_v, u32 n, u32 shift, u32 mask,
+                       const u32* bstart, u32* status, u32* tile_counter, cudaStream_t s);
+
+// Bucketed sort + collect (lnt_bucket.cu): applies to n >= 2^20 pairs whose
+// keys have at most 28 bits below the bucket bits.
+bool bucket_path_applies(size_t n, int key_bits);
+size_t bucket_ctrl_bytes(size_t n);
+int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int skip_zero_heads, u64* k0, double* v0,
+                             u64* k1, double* v1, void* ctrl, u64* out_k, double* out_v, u64* d_nout,
+                             cudaStream_t s, bool* used);
+
 }  // namespace lnt

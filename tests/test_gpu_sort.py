@@ -175,3 +175,35 @@ def test_sort_merge_matches_oracle(cuda, torch, rng, dims, na, nb, op):
     np.testing.assert_array_equal(ek, c.keys)
     assert rel_ok(to_host(v), c.vals, ea)
     assert cuda.device_status() == 0
+
+
+@pytest.mark.parametrize("path", ["bucketed", "lsd"])
+@pytest.mark.parametrize("dims,n_each,dup_frac", [([512] * 4, 1 << 20, 0.0), ([64] * 4, 1 << 20, 0.0),
+                                                   ([512] * 4, 3 << 19, 0.0), ([512] * 4, 1 << 20, 0.5)])
+def test_sort_merge_both_paths(cuda, torch, rng, monkeypatch, path, dims, n_each, dup_frac):
+    """The bucketed sort+collect (hist, 2 passes, per-bucket shared-memory sort
+    with fused collect) and the LSD path give identical results; heavily
+    duplicated keys overflow a bucket and fall back to the LSD path."""
+    import libnt_b200 as L
+    if path == "lsd":
+        monkeypatch.setenv("LNT_NO_BUCKETS", "1")
+    ak, av, bk, bv = _merge_case(rng, dims, n_each, n_each, zero_frac=0.1)
+    if dup_frac:
+        ak[: int(n_each * dup_frac)] = ak[0]
+    # the smallest key gets only zero values: it must survive (position 0)
+    total = int(np.prod(dims))
+    ak[1], av[1] = 0, 0.0
+    bk[1], bv[1] = 0, 0.0
+    spec = L.RekeySpec.make(dims, [0, 1, 2, 3], [3, 2, 1, 0])
+    k, v = cuda.sort_reduce(to_dev(ak, torch), to_dev(av, torch), to_dev(bk, torch), to_dev(bv, torch),
+                            max_key=total, a_rekey=spec)
+    allk = np.concatenate([oracle.rekey(ak, dims, [0, 1, 2, 3], [3, 2, 1, 0]), bk])
+    allv = np.concatenate([av, bv])
+    sk, sv = oracle.sort_pairs(allk, allv)
+    ek, ev, ea = oracle.collect_duplicates(sk, sv, with_abs=True)
+    np.testing.assert_array_equal(to_host(k, np.uint64), ek)
+    if dup_frac:  # a run spanning many tiles is summed tile-wise on the LSD fallback
+        assert rel_ok(to_host(v), ev, ea)
+    else:  # same stable order and sequential fold: identical sums
+        np.testing.assert_array_equal(to_host(v), ev)
+    assert cuda.device_status() == 0
