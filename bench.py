@@ -726,6 +726,181 @@ def run_dense(args):
     })), flush=True)
     return 0
 
+SKEW_DIMS = (1024, 1024, 256, 256, 4096)  # a(i,j,k,l), b(k,l,m)
+
+
+def _zipf_cdf(dim, xp, **kw):
+    p = xp.arange(1, dim + 1, **kw) ** -1.1
+    return xp.cumsum(p / p.sum(), 0)
+
+
+def skewed_inputs_gpu(dev, nnz_a, nnz_b, dims=SKEW_DIMS, seed=0):
+    """c(i,j,m) = a(i,j,k,l) * b(k,l,m): (k,l) ~ Zipf(1.1) truncated to the mode
+    extent, rank r -> coordinate r-1 in both operands (aligned), i, j, m uniform,
+    values N(0,1), duplicate coordinates collapsed.  Returned as key-sorted
+    lattices A (rows (i,j), cols (k,l)) and B (rows (k,l), cols m)."""
+    import torch
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    di, dj, dk, dl, dm = dims
+
+    def zipf(n, dim):
+        cdf = _zipf_cdf(dim, torch, dtype=torch.float64, device=dev)
+        u = torch.rand(n, generator=g, device=dev, dtype=torch.float64)
+        return torch.searchsorted(cdf, u).clamp_(max=dim - 1)
+
+    i = torch.randint(0, di, (nnz_a,), generator=g, device=dev)
+    j = torch.randint(0, dj, (nnz_a,), generator=g, device=dev)
+    ak = torch.unique((i + di * j) + (di * dj) * (zipf(nnz_a, dk) + dk * zipf(nnz_a, dl)))
+    del i, j
+    kb, lb = zipf(nnz_b, dk), zipf(nnz_b, dl)
+    m = torch.randint(0, dm, (nnz_b,), generator=g, device=dev)
+    bk = torch.unique((kb + dk * lb) + (dk * dl) * m)
+    del kb, lb, m
+    av = torch.randn(ak.numel(), generator=g, device=dev, dtype=torch.float64)
+    bv = torch.randn(bk.numel(), generator=g, device=dev, dtype=torch.float64)
+    return ak, av, bk, bv
+
+
+def skewed_inputs_cpu(nnz_a, nnz_b, dims=SKEW_DIMS, seed=0):
+    """The same distributions drawn with numpy (for the CPU baseline sample)."""
+    rng = np.random.default_rng(seed)
+    di, dj, dk, dl, dm = dims
+
+    def zipf(n, dim):
+        return np.minimum(np.searchsorted(_zipf_cdf(dim, np, dtype=np.float64), rng.random(n)), dim - 1)
+
+    i, j = rng.integers(0, di, nnz_a), rng.integers(0, dj, nnz_a)
+    ak = np.unique((i + di * j) + (di * dj) * (zipf(nnz_a, dk) + dk * zipf(nnz_a, dl))).astype(np.uint64)
+    bk = np.unique((zipf(nnz_b, dk) + dk * zipf(nnz_b, dl)) + (dk * dl) * rng.integers(0, dm, nnz_b)).astype(
+        np.uint64)
+    return ak, rng.standard_normal(ak.size), bk, rng.standard_normal(bk.size)
+
+
+def run_skewed(args):
+    """Large skewed sparse contraction c(i,j,m) = a(i,j,k,l) * b(k,l,m) on
+    key-sorted lattices; a step = lnt_lattice_mult_plan (product count) +
+    lnt_lattice_mult (the tile engine at this shape) through the C ABI."""
+    import ctypes as C
+
+    import torch
+
+    import libnt_b200 as L
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dims = tuple(int(x) for x in args.skew_dims.split(","))
+    di, dj, dk, dl, dm = dims
+    h, w, wB = di * dj, dk * dl, dm
+    nnz = 1 << args.skew_log2
+    ak, av, bk, bv = skewed_inputs_gpu(dev, nnz, nnz, dims)
+    A = L.Lattice.of(ak, av, h, w, 1)
+    B = L.Lattice.of(bk, bv, w, wB, 1)
+    lib = L.lib()
+    nb_ = C.c_size_t(0)
+    L._check(lib.lnt_lattice_mult_plan_workspace(C.byref(A), C.byref(B), C.byref(nb_)), "plan_workspace")
+    plan = L.workspace(nb_.value, dev)
+    counts = torch.zeros(2, dtype=torch.int64, device=dev)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def run_plan():
+        L._check(lib.lnt_lattice_mult_plan(C.byref(A), C.byref(B), C.c_void_p(plan.data_ptr()), plan.numel(),
+                                           C.c_void_p(counts.data_ptr()), stream), "lnt_lattice_mult_plan")
+
+    run_plan()
+    products, cap = (int(x) for x in counts.tolist())
+    L._check(lib.lnt_lattice_mult_workspace(C.byref(A), C.byref(B), C.c_uint64(products), C.byref(nb_)),
+             "lnt_lattice_mult_workspace")
+    ws = L.workspace(nb_.value, dev)
+    ck = torch.empty(max(cap, 1), dtype=torch.int64, device=dev)
+    cv = torch.empty(max(cap, 1), dtype=torch.float64, device=dev)
+    nc = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    def step():
+        run_plan()
+        L._check(lib.lnt_lattice_mult(C.byref(A), C.byref(B), C.c_void_p(plan.data_ptr()), C.c_uint64(products),
+                                      C.c_void_p(ws.data_ptr()), ws.numel(), C.c_void_p(ck.data_ptr()),
+                                      C.c_void_p(cv.data_ptr()), C.c_void_p(nc.data_ptr()), stream),
+                 "lnt_lattice_mult")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    n_out = int(nc.item())
+    assert L.device_status() == 0
+    assert 0 < n_out <= cap, (n_out, cap)
+    # spot check: 64 output entries (exact integer positions) against a float64 recomputation from the inputs
+    sel = torch.from_numpy((np.arange(64, dtype=np.int64) * (n_out - 1)) // 63).to(dev)
+    keys, vals = ck[sel].cpu().numpy(), cv[sel].cpu().numpy()
+    akh, avh, bkh, bvh = (x.cpu().numpy() for x in (ak, av, bk, bv))
+    a_col, a_row = akh // h, akh % h
+    spot = 0.0
+    for key, val in zip(keys, vals):
+        r, col = int(key) % h, int(key) // h
+        sa = a_row == r
+        cs, va = a_col[sa], avh[sa]
+        bpos = np.searchsorted(bkh, cs + w * col)
+        hit = (bpos < bkh.size) & (bkh[np.minimum(bpos, bkh.size - 1)] == cs + w * col)
+        terms = va[hit] * bvh[bpos[hit]]
+        assert hit.any()
+        spot = max(spot, abs(val - terms.sum()) / max(np.abs(terms).sum(), 1e-300))
+    assert spot <= 1e-12, spot
+    launches0 = L.launch_count()
+    L.profile_reset()
+    L.profile_enable(True)
+    sampler = ClockSampler(torch.cuda.current_device())
+    e0, e1 = _events()
+    with sampler:
+        torch.cuda.synchronize()
+        barrier(world)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    L.profile_enable(False)
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    launches = L.launch_count() - launches0
+    names = ("spgemm_colptr", "spgemm_count", "sort_hist", "sort_onesweep", "collect", "tile_rowptr", "tile_bprep",
+             "tile_cbits", "tile_count", "tile_scan", "tile_numeric")
+    kernels = {k: L.profile_query(k)[0] / args.steps for k in names}
+    if rank != 0:
+        return 0
+    peak, peak_kind = peaks()
+    alg = 16.0 * (ak.numel() + bk.numel() + n_out)
+    num_ms = kernels["tile_numeric"]
+    cpu = None
+    if not args.no_cpu and world == 1:
+        import oracle
+        sample_log2 = args.skew_cpu_log2
+        cak, cav, cbk, cbv = skewed_inputs_cpu(1 << sample_log2, 1 << sample_log2, dims)
+        t0 = time.perf_counter()
+        ok, _ = oracle.lattice_mult(cak, cav, h, w, 1, cbk, cbv, wB)
+        t = time.perf_counter() - t0
+        a_cnt = np.bincount((cak // h).astype(np.int64), minlength=w)
+        b_cnt = np.bincount((cbk % w).astype(np.int64), minlength=w)
+        p_cpu = int((a_cnt * b_cnt).sum())
+        cpu = {"value": p_cpu / t, "unit": "products/s", "cores": 1, "kind": "port",
+               "sample": f"same dims and distributions at 2^{sample_log2} nnz per operand ({p_cpu:.3e} products, "
+                         f"{ok.size} output nnz): restated csc_no_accum (per-column scatter, sort, fold), one thread; "
+                         "products/s is normalised by that sample's product count"}
+    config = {"workload": f"skewed sparse contraction c(i,j,m)=a(i,j,k,l)*b(k,l,m), a dims {di}x{dj}x{dk}x{dl}, "
+                          f"b dims {dk}x{dl}x{dm}, 2^{args.skew_log2} coordinates drawn per operand "
+                          "(duplicates collapsed), (k,l) Zipf(1.1) aligned, values N(0,1); step = plan + tile-engine "
+                          "product on key-sorted lattices",
+              "nnz_a": int(ak.numel()), "nnz_b": int(bk.numel()), "products": products, "output_nnz": n_out,
+              "l2": "output (16 B x output nnz) far larger than L2", "parallelism": "1 GPU"}
+    print(json.dumps(_line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
+        "gpu_launches": launches, "kernels_ms_per_step": kernels, "spot_check_max_rel_err": spot,
+        "roofline": {"bound": "hbm", "kernel": "tile_numeric (products, staging, output write)",
+                     "achieved": alg / (num_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (num_ms * 1e-3) / 1e9 / peak, "alg_bytes_per_launch": alg,
+                     "avg_launch_ms": num_ms, "peak_source": peak_kind,
+                     "step_frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None},
+        "cpu_baseline": cpu, "clocks": sampler.summary(),
+    })), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -736,13 +911,17 @@ def main():
     ap.add_argument("--nnz-log2", type=int, default=26,
                     help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
-    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense"],
+    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed"],
                     help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
                          "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")
     ap.add_argument("--slices", type=int, default=7, help="dense scheme I: INT8 slices per operand")
     ap.add_argument("--moduli", type=int, default=13, help="dense scheme II: moduli (uniform data)")
     ap.add_argument("--no-scheme1", action="store_true", help="dense: skip timing scheme I")
     ap.add_argument("--dense-log2", type=int, default=14, help="dense: log2 of the GEMM size (14 = the workload)")
+    ap.add_argument("--skew-log2", type=int, default=25, help="skewed: log2 of coordinates drawn per operand")
+    ap.add_argument("--skew-dims", default=",".join(map(str, SKEW_DIMS)),
+                    help="skewed: i,j,k,l,m extents (default: the workload's)")
+    ap.add_argument("--skew-cpu-log2", type=int, default=18, help="skewed: CPU baseline sample size (log2 nnz)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -752,7 +931,7 @@ def main():
             return 0
         return run_reference(args)
     return {"merge": run_ours, "contraction": run_contraction, "batched": run_batched,
-            "dense": run_dense}[args.workload](args)
+            "dense": run_dense, "skewed": run_skewed}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -20,7 +20,18 @@
 //
 // ESC engine (any shape): expand all P products (key, a*b) load-balanced by
 // product index, radix-sort them by key, fold duplicates (no zero skipping).
+//
+// Tile engine (lnt_tile.cu): products whose output is dense or nearly so.
+//
+// Engine choice (lnt_lattice_mult_workspace and lnt_lattice_mult, from the
+// shape and the product count P): SPA when h <= 1024; else the tile engine
+// when its bitmaps fit and P >= 2^30 or P >= (nnz(A) + h*d) * ceil(wB/64)
+// (the tile engine's work per 64-column tile is one pass over A's entries);
+// else ESC.  LNT_SPGEMM_ENGINE=tile|esc in the environment forces an engine
+// (tile only where its bitmaps fit).
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 
 #include "lnt_scan.cuh"
 #include "lnt_sort.cuh"
@@ -30,6 +41,11 @@ namespace lnt {
 int run_collect(const u64* keys, const double* vals, size_t n, int skip_zero_heads, u64* out_k, double* out_v,
                 u64* d_nout, void* ws, cudaStream_t s);
 size_t collect_workspace_bytes(size_t n);
+bool tile_shape_ok(u64 h, u64 w, u64 wB, u64 d, u64 na, u64 nb);
+size_t tile_workspace_bytes(u64 h, u64 w, u64 wB, u64 d, u64 na, u64 nb);
+int run_tile_mult(const u64* akeys, const double* avals, u64 na, const u64* bkeys, const double* bvals, u64 nb,
+                  u64 h, u64 w, u64 wB, u64 d, void* ws, size_t ws_bytes, u64* ck, double* cv, u64* d_nc,
+                  cudaStream_t s);
 
 namespace {
 
@@ -250,6 +266,24 @@ PlanLayout plan_layout(const Shape& s) {
 
 bool spa_eligible(const Shape& s) { return s.h <= (u64)kSpaMaxRows && s.dense_a && s.dense_b; }
 
+enum class Engine { Spa, Esc, Tile };
+
+Engine choose_engine(const Shape& s, u64 products) {
+  const bool tile_ok = tile_shape_ok(s.h, s.w, s.wB, s.d, s.A.nnz, s.B.nnz);
+  if (const char* e = std::getenv("LNT_SPGEMM_ENGINE")) {
+    if (!std::strcmp(e, "tile") && tile_ok) return Engine::Tile;
+    if (!std::strcmp(e, "esc")) return Engine::Esc;
+  }
+  if (spa_eligible(s)) return Engine::Spa;
+  const u64 nt = (s.wB + 63) / 64;
+  if (tile_ok && (products >= (1ull << 30) || products >= (s.A.nnz + s.h * s.d) * nt)) return Engine::Tile;
+  return Engine::Esc;
+}
+
+// counts[1] = min(counts[0], dense): the output holds at most one entry per
+// (row, col, tab) and at most one per product.
+__global__ void capacity_kernel(u64* counts, u64 dense) { counts[1] = min(counts[0], dense); }
+
 int grid_for(u64 work, int threads, int per_sm = 8) {
   const u64 want = (work + threads - 1) / threads;
   const u64 cap = (u64)sm_count() * per_sm;
@@ -316,9 +350,8 @@ int lnt_lattice_mult_plan(const lnt_lattice* a, const lnt_lattice* b, void* plan
                    p + L.off_scan, cs, "spgemm_scan");
     if (st != LNT_OK) return st;
   } else {
-    // output bound: the product count
-    if (cudaMemcpyAsync(d_counts + 1, d_counts, 8, cudaMemcpyDeviceToDevice, cs) != cudaSuccess)
-      return LNT_DEVICE_ERROR;
+    capacity_kernel<<<1, 1, 0, cs>>>((u64*)d_counts, s.h * s.wB * s.d);
+    count_launch();
   }
   return launch_status();
 }
@@ -328,8 +361,13 @@ int lnt_lattice_mult_workspace(const lnt_lattice* a, const lnt_lattice* b, uint6
   int st = check_shape(a, b, &s);
   if (st != LNT_OK) return st;
   if (!bytes) return LNT_BAD_ARG;
-  if (spa_eligible(s)) {
+  const Engine eng = choose_engine(s, products);
+  if (eng == Engine::Spa) {
     *bytes = 256;
+    return LNT_OK;
+  }
+  if (eng == Engine::Tile) {
+    *bytes = tile_workspace_bytes(s.h, s.w, s.wB, s.d, s.A.nnz, s.B.nnz);
     return LNT_OK;
   }
   if (products >= (1ull << 30)) return LNT_UNSUPPORTED;
@@ -363,7 +401,11 @@ int lnt_lattice_mult(const lnt_lattice* a, const lnt_lattice* b, const void* pla
   if (st != LNT_OK) return st;
   if (workspace_bytes < need || (need > 256 && !workspace)) return LNT_WORKSPACE;
   if (products && (!c_keys || !c_vals)) return LNT_BAD_ARG;
-  if (spa_eligible(s)) {
+  const Engine eng = choose_engine(s, products);
+  if (eng == Engine::Tile)
+    return run_tile_mult(s.A.keys, s.A.vals, s.A.nnz, s.B.keys, s.B.vals, s.B.nnz, s.h, s.w, s.wB, s.d, workspace,
+                         workspace_bytes, (u64*)c_keys, c_vals, (u64*)d_nc, cs);
+  if (eng == Engine::Spa) {
     {
       ProfScope prof("spgemm_spa_numeric", cs);
       spa_kernel<true><<<grid_for(L.units * 32, kSpaWarps * 32), kSpaWarps * 32, 0, cs>>>(
