@@ -792,7 +792,8 @@ def run_skewed(args):
     di, dj, dk, dl, dm = dims
     h, w, wB = di * dj, dk * dl, dm
     nnz = 1 << args.skew_log2
-    ak, av, bk, bv = skewed_inputs_gpu(dev, nnz, nnz, dims)
+    nnz_b = 1 << (args.skew_b_log2 if args.skew_b_log2 is not None else args.skew_log2)
+    ak, av, bk, bv = skewed_inputs_gpu(dev, nnz, nnz_b, dims)
     A = L.Lattice.of(ak, av, h, w, 1)
     B = L.Lattice.of(bk, bv, w, wB, 1)
     lib = L.lib()
@@ -884,7 +885,7 @@ def run_skewed(args):
                          f"{ok.size} output nnz): restated csc_no_accum (per-column scatter, sort, fold), one thread; "
                          "products/s is normalised by that sample's product count"}
     config = {"workload": f"skewed sparse contraction c(i,j,m)=a(i,j,k,l)*b(k,l,m), a dims {di}x{dj}x{dk}x{dl}, "
-                          f"b dims {dk}x{dl}x{dm}, 2^{args.skew_log2} coordinates drawn per operand "
+                          f"b dims {dk}x{dl}x{dm}, {nnz} / {nnz_b} coordinates drawn for a / b "
                           "(duplicates collapsed), (k,l) Zipf(1.1) aligned, values N(0,1); step = plan + tile-engine "
                           "product on key-sorted lattices",
               "nnz_a": int(ak.numel()), "nnz_b": int(bk.numel()), "products": products, "output_nnz": n_out,
@@ -919,6 +920,8 @@ def main():
     ap.add_argument("--no-scheme1", action="store_true", help="dense: skip timing scheme I")
     ap.add_argument("--dense-log2", type=int, default=14, help="dense: log2 of the GEMM size (14 = the workload)")
     ap.add_argument("--skew-log2", type=int, default=25, help="skewed: log2 of coordinates drawn per operand")
+    ap.add_argument("--skew-b-log2", type=int, default=None, help="skewed: log2 of coordinates drawn for b "
+                                                                   "(default: --skew-log2)")
     ap.add_argument("--skew-dims", default=",".join(map(str, SKEW_DIMS)),
                     help="skewed: i,j,k,l,m extents (default: the workload's)")
     ap.add_argument("--skew-cpu-log2", type=int, default=18, help="skewed: CPU baseline sample size (log2 nnz)")

@@ -11,20 +11,29 @@
 //   B row-major: B re-keyed to j + wB*(c + w*t), sorted, duplicate keys
 //     summed, with row pointers (w*d + 1); a row holding at least a quarter of
 //     its columns is also expanded into a dense row of Bd (one slot per such
-//     row, zero-filled, padded to whole 64-column tiles); for every row
-//     tp[row][q] = entries of the row left of column 64q (q = 0..nt);
+//     row, zero-filled, padded to whole 128-column tiles); for every row
+//     tp[row][q] = position in B of the row's first entry at or right of
+//     column 128q (q = 0..nt);
+//   A records: per A entry its B row (c + w*t), that row's dense slot and the
+//     value, 16 bytes, so one load per entry serves every tile;
 //   bitmaps, one bit per (row, column), 64-column words: Bbits (B rows) and
 //     Cbits (C rows, = OR of the Bbits rows that A row selects) — the output
 //     pattern, computed before any arithmetic.
-// Output positions: per (tab, column, panel of 128 rows) the number of
+// Output positions: per (tab, column, panel of 64 rows) the number of
 // pattern bits, exclusive-scanned in (tab, column, panel) order, so each
 // panel's rows of one column land at a known contiguous offset.
-// Numeric pass: one CTA per (panel, 64-column tile) unit, one warp per row,
-// two columns per lane in registers; per A entry of the row a dense B row
-// adds one coalesced 512-byte load, a sparse one its tile segment (OR-reduced
-// column mask, lanes pick their entries by shuffle).  The 128 x 64 tile is
-// staged in shared memory and written column by column (contiguous runs).
+// Numeric pass: one CTA per (panel, 128-column tile) unit; warps take rows
+// from a shared counter, four columns per lane in registers.  Each 32-entry
+// chunk of the row's A records is split by ballot into per-warp shared lists
+// of dense-row items (Bd position, value) and sparse-row items (segment,
+// value), so the inner loops read one broadcast shared-memory item per entry:
+// a dense item adds two coalesced 512-byte loads and four FMAs (several items'
+// loads issued before their FMAs), a sparse item's segment is scattered by
+// the lanes into a per-warp shared accumulator row (distinct columns within
+// a segment).  The 64 x 128 tile is staged in shared memory and written
+// column by column (contiguous runs).
 #include <algorithm>
+#include <cstdlib>
 
 #include "lnt_scan.cuh"
 #include "lnt_sort.cuh"
@@ -38,17 +47,39 @@ size_t collect_workspace_bytes(size_t n);
 namespace {
 
 constexpr u32 FULL = 0xffffffffu;
-constexpr int kTileCols = 64;      // output columns per tile (two per lane)
-constexpr int kPanelRows = 128;    // output rows per unit
-constexpr int kTileThreads = 512;  // 16 warps, 8 rows each
+constexpr int kWordCols = 64;      // columns per bitmap word
+constexpr int kTileCols = 128;     // output columns per numeric tile (four per lane)
+constexpr int kPanelRows = 64;     // output rows per unit
+constexpr int kTileThreads = 512;  // 16 warps
+constexpr int kTileWarps = kTileThreads / 32;
 constexpr int kTileGroup = 8;      // tiles of one panel processed by consecutive units
-constexpr int kStageStride = 65;   // doubles per staged row
+constexpr int kStageStride = 129;  // doubles per staged row
+constexpr int kDenseBatch = 2;     // dense items whose loads are issued before their FMAs (LNT_TILE_BATCH=4: four)
+
+struct ARec {
+  u32 br;    // B row c + w*t
+  int slot;  // its dense slot, or -1
+  double v;
+};
+struct DenseItem {
+  u64 pos;   // double2 index of the item's tile in Bd
+  double v;
+};
+struct SparseItem {
+  u64 s0;    // first entry of the segment in row-major B
+  double v;
+  u64 kb;    // key of the tile's column 0 in that B row
+  u32 len;
+  u32 pad;
+};
 constexpr size_t kStageBytes = (size_t)kPanelRows * kStageStride * 8;
+constexpr size_t kNumericSmem = kStageBytes + (size_t)kTileWarps * 32 * (sizeof(DenseItem) + sizeof(SparseItem)) +
+                                (size_t)kTileWarps * kTileCols * 8;
 constexpr size_t kMaxBitmapBytes = 16ull << 30;
 
 struct TileDims {
   u64 h, w, wB, d;
-  u32 nt, np;  // 64-column tiles per row, 128-row panels per tab
+  u32 nt, nw, np;  // 128-column tiles per row, 64-column bitmap words per row, 64-row panels per tab
   u64 smax;    // dense-row slots
 };
 
@@ -59,6 +90,7 @@ TileDims tile_dims(u64 h, u64 w, u64 wB, u64 d, u64 nb) {
   t.wB = wB;
   t.d = d;
   t.nt = (u32)((wB + kTileCols - 1) / kTileCols);
+  t.nw = (u32)((wB + kWordCols - 1) / kWordCols);
   t.np = (u32)((h + kPanelRows - 1) / kPanelRows);
   const u64 thr = std::max<u64>(wB, kTileCols);  // dense: 4 * len >= thr
   t.smax = std::min<u64>(w * d, 4 * nb / thr);
@@ -66,7 +98,8 @@ TileDims tile_dims(u64 h, u64 w, u64 wB, u64 d, u64 nb) {
 }
 
 struct TileLayout {
-  size_t ctrl, ak, av, tk, tv, bk, bv, arow, brow, dslot, tp, bbits, bd, cbits, cnt, base, scan, coll, misc, total;
+  size_t ctrl, ak, av, tk, tv, bk, bv, arow, brow, dslot, tp, bbits, bd, cbits, cnt, base, scan, coll, arec, misc,
+      total;
   SortPlan pa, pb;
 };
 
@@ -92,14 +125,15 @@ TileLayout tile_layout(const TileDims& t, u64 na, u64 nb) {
   L.arow = take((t.h * t.d + 1) * 8);
   L.brow = take((t.w * t.d + 1) * 8);
   L.dslot = take(t.w * t.d * 4);
-  L.tp = take(t.w * t.d * (u64)(t.nt + 1) * 4);
-  L.bbits = take(t.w * t.d * (u64)t.nt * 8);
+  L.tp = take(t.w * t.d * (u64)(t.nt + 1) * 8);
+  L.bbits = take(t.w * t.d * (u64)t.nw * 8);
   L.bd = take(t.smax * (u64)t.nt * kTileCols * 8);
-  L.cbits = take(t.h * t.d * (u64)t.nt * 8);
+  L.cbits = take(t.h * t.d * (u64)t.nw * 8);
   L.cnt = take(ncnt * 4);
   L.base = take((ncnt + 1) * 8);
   L.scan = take(scan::workspace_bytes(ncnt));
   L.coll = take(collect_workspace_bytes(nb));
+  L.arec = take(na * sizeof(ARec));
   L.misc = take(256);  // [0] unique B count, [1] slot counter
   L.total = off;
   return L;
@@ -133,44 +167,70 @@ __global__ void tile_slot_kernel(const u64* __restrict__ brow, u64 nrows, u64 th
   }
 }
 
+// tp[row][*] = brow[row] for rows without entries (their segments are empty).
+__global__ void tile_tp_empty_kernel(const u64* __restrict__ brow, u64 nrows, u32 nt, u64* __restrict__ tp) {
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += stride) {
+    const u64 rs = brow[r];
+    if (brow[r + 1] != rs) continue;
+    for (u32 q = 0; q <= nt; ++q) tp[r * (u64)(nt + 1) + q] = rs;
+  }
+}
+
+// A record per A entry (row-major order).
+__global__ void tile_arec_kernel(const u64* __restrict__ ak, const double* __restrict__ av, u64 na, u64 w,
+                                 Divider div_w, Divider div_h, const int* __restrict__ dslot, ARec* __restrict__ rec) {
+  const u64 stride = (u64)gridDim.x * blockDim.x;
+  for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < na; e += stride) {
+    const u64 k = ak[e];
+    const u64 row = divide(k, div_w);  // r + h*t
+    const u64 br = k - row * w + w * divide(row, div_h);
+    ARec r;
+    r.br = (u32)br;
+    r.slot = dslot[br];
+    r.v = av[e];
+    rec[e] = r;
+  }
+}
+
 // Per unique B entry: its bit in Bbits, its value in Bd (dense rows), and the
 // tile pointers of its row.
 __global__ void tile_bentry_kernel(const u64* __restrict__ bk, const double* __restrict__ bv,
                                    const u64* __restrict__ d_n, const u64* __restrict__ brow, Divider div_wB, u64 wB,
-                                   u32 nt, const int* __restrict__ dslot, u64* __restrict__ bbits,
-                                   u32* __restrict__ tp, double* __restrict__ bd) {
+                                   u32 nt, u32 nw, const int* __restrict__ dslot, u64* __restrict__ bbits,
+                                   u64* __restrict__ tp, double* __restrict__ bd) {
   const u64 n = *d_n;
   const u64 stride = (u64)gridDim.x * blockDim.x;
   for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
     const u64 k = bk[e];
     const u64 row = divide(k, div_wB);
     const u64 j = k - row * wB;
-    const u32 q = (u32)(j >> 6);
-    atomicOr(reinterpret_cast<unsigned long long*>(bbits + row * nt + q), 1ull << (j & 63));
+    const u32 q = (u32)(j / kTileCols);
+    atomicOr(reinterpret_cast<unsigned long long*>(bbits + row * nw + j / kWordCols), 1ull << (j % kWordCols));
     const int slot = dslot[row];
     if (slot >= 0) bd[(u64)slot * nt * kTileCols + j] = bv[e];
     const u64 rs = brow[row], re = brow[row + 1];
-    u32* t = tp + row * (u64)(nt + 1);
+    u64* t = tp + row * (u64)(nt + 1);
     long long qprev = -1;
-    if (e > rs) qprev = (long long)((bk[e - 1] - row * wB) >> 6);
-    for (long long qq = qprev + 1; qq <= (long long)q; ++qq) t[qq] = (u32)(e - rs);
+    if (e > rs) qprev = (long long)((bk[e - 1] - row * wB) / kTileCols);
+    for (long long qq = qprev + 1; qq <= (long long)q; ++qq) t[qq] = e;
     if (e + 1 == re)
-      for (u32 qq = q + 1; qq <= nt; ++qq) t[qq] = (u32)(e + 1 - rs);
+      for (u32 qq = q + 1; qq <= nt; ++qq) t[qq] = e + 1;
   }
 }
 
 // Cbits[row] = OR of Bbits[c + w*t] over the A entries (row, c); warp per row.
 __global__ void tile_cbits_kernel(const u64* __restrict__ ak, const u64* __restrict__ arow,
-                                  const u64* __restrict__ bbits, u64 h, u64 w, u64 d, u32 nt, Divider div_h,
+                                  const u64* __restrict__ bbits, u64 h, u64 w, u64 d, u32 nw, Divider div_h,
                                   u64* __restrict__ cbits) {
   const int lane = threadIdx.x & 31;
   const u64 nrows = h * d;
-  const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
-  for (u64 row = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrows; row += nw) {
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 row = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrows; row += nwarps) {
     const u64 t = divide(row, div_h);
     const u64 e0 = arow[row], e1 = arow[row + 1];
     const u64 cbase = w * t - w * row;  // B row = A key + cbase
-    for (u32 w0 = 0; w0 < nt; w0 += 32) {
+    for (u32 w0 = 0; w0 < nw; w0 += 32) {
       const u32 word = w0 + lane;
       u64 acc = 0;
       for (u64 eb = e0; eb < e1; eb += 32) {
@@ -179,18 +239,19 @@ __global__ void tile_cbits_kernel(const u64* __restrict__ ak, const u64* __restr
         const int n = (int)(e1 - eb < 32 ? e1 - eb : 32);
         for (int k = 0; k < n; ++k) {
           const u64 b = __shfl_sync(FULL, br, k);
-          if (word < nt) acc |= bbits[b * nt + word];
+          if (word < nw) acc |= bbits[b * nw + word];
         }
       }
-      if (word < nt) cbits[row * nt + word] = acc;
+      if (word < nw) cbits[row * nw + word] = acc;
     }
   }
 }
 
 // cnt[(t*wB + col)*np + p] = pattern bits of column col among panel p's rows;
-// warp per (t, p, q).
+// warp per (t, p, bitmap word q).
 __global__ void tile_count_kernel(const u64* __restrict__ cbits, u64 h, u64 wB, u64 d, u32 nt, u32 np,
                                   u32* __restrict__ cnt) {
+  // here nt counts bitmap words per row
   const int lane = threadIdx.x & 31;
   const u64 units = d * np * (u64)nt;
   const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
@@ -213,7 +274,7 @@ __global__ void tile_count_kernel(const u64* __restrict__ cbits, u64 h, u64 wB, 
         }
       }
     }
-    const u64 c0 = (u64)q * kTileCols + lane, c1 = c0 + 32;
+    const u64 c0 = (u64)q * kWordCols + lane, c1 = c0 + 32;
     if (c0 < wB) cnt[(t * wB + c0) * np + p] = clo;
     if (c1 < wB) cnt[(t * wB + c1) * np + p] = chi;
   }
@@ -225,28 +286,37 @@ struct CountGet {
 };
 
 struct NumArgs {
-  const u64* ak;
-  const double* av;
+  const ARec* rec;
   const u64* arow;
   const u64* bk;
   const double* bv;
-  const u64* brow;
-  const int* dslot;
-  const u32* tp;
+  const u64* tp;
   const double* bd;
   const u64* cbits;
   const unsigned long long* base;
   u64 h, w, wB, d;
-  u32 nt, np;
+  u32 nt, nw, np;
   u64 units;
   u64* ck;
   double* cv;
 };
 
+template <int BATCH>
 __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a) {
-  extern __shared__ double stage[];  // [kPanelRows][kStageStride]
-  __shared__ u64 s_bits[kPanelRows];
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* stage = reinterpret_cast<double*>(smem);  // [kPanelRows][kStageStride]
+  DenseItem* dlist = reinterpret_cast<DenseItem*>(smem + kStageBytes);
+  SparseItem* slist = reinterpret_cast<SparseItem*>(dlist + kTileWarps * 32);
+  double* sacc_all = reinterpret_cast<double*>(slist + kTileWarps * 32);
+  __shared__ u64 s_bits[kPanelRows][2];
+  __shared__ u32 s_next;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  DenseItem* dl = dlist + warp * 32;
+  SparseItem* sl = slist + warp * 32;
+  double* sacc = sacc_all + warp * kTileCols;
+  for (int c = lane; c < kTileCols; c += 32) sacc[c] = 0.0;
+  const u32 lt = (1u << lane) - 1u;
+  const double2* bd2 = reinterpret_cast<const double2*>(a.bd);
   const u64 per_tab = (u64)a.np * a.nt;
   for (u64 u = blockIdx.x; u < a.units; u += gridDim.x) {
     const u64 t = u / per_tab;
@@ -257,78 +327,111 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
     const u32 p = (u32)(within / gs);
     const u32 q = (u32)(qg * kTileGroup + (within - (u64)p * gs));
     const u64 row0 = (u64)p * kPanelRows;
-    if (threadIdx.x < kPanelRows) {
-      const u64 r = row0 + threadIdx.x;
-      s_bits[threadIdx.x] = r < a.h ? a.cbits[(r + a.h * t) * a.nt + q] : 0ull;
+    if (threadIdx.x < 2 * kPanelRows) {
+      const u64 r = row0 + (threadIdx.x >> 1);
+      const u32 word = 2 * q + (threadIdx.x & 1);
+      s_bits[threadIdx.x >> 1][threadIdx.x & 1] = r < a.h && word < a.nw ? a.cbits[(r + a.h * t) * a.nw + word] : 0ull;
     }
+    if (threadIdx.x == 0) s_next = 0;
     __syncthreads();
-    const double2* bd2 = reinterpret_cast<const double2*>(a.bd);
-    for (int i = warp; i < kPanelRows; i += kTileThreads / 32) {
-      if (s_bits[i] == 0ull) continue;
+    for (;;) {
+      u32 i = 0;
+      if (lane == 0) i = atomicAdd(&s_next, 1u);
+      i = __shfl_sync(FULL, i, 0);
+      if (i >= (u32)kPanelRows) break;
+      if ((s_bits[i][0] | s_bits[i][1]) == 0ull) continue;
       const u64 row = row0 + i + a.h * t;
       const u64 e0 = a.arow[row], e1 = a.arow[row + 1];
-      const u64 cbase = a.w * t - a.w * row;  // B row = A key + cbase
-      double acc0 = 0.0, acc1 = 0.0;
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+      bool had_sparse = false;
       for (u64 eb = e0; eb < e1; eb += 32) {
         const u64 e = eb + lane;
-        u64 br = 0, s0 = 0;
-        double v = 0.0;
-        int slot = -1;
+        ARec rc;
+        rc.br = 0;
+        rc.slot = -1;
+        rc.v = 0.0;
+        if (e < e1) rc = a.rec[e];
+        u64 s0 = 0;
         u32 len = 0;
-        if (e < e1) {
-          br = a.ak[e] + cbase;
-          v = a.av[e];
-          slot = a.dslot[br];
-          if (slot < 0) {
-            const u32* tpr = a.tp + br * (u64)(a.nt + 1);
-            const u32 lo = tpr[q];
-            len = tpr[q + 1] - lo;
-            s0 = a.brow[br] + lo;
+        if (e < e1 && rc.slot < 0) {
+          const u64* tpr = a.tp + (u64)rc.br * (a.nt + 1) + q;
+          s0 = tpr[0];
+          len = (u32)(tpr[1] - s0);
+        }
+        const bool dense = e < e1 && rc.slot >= 0;
+        const u32 dm = __ballot_sync(FULL, dense);
+        const u32 sm = __ballot_sync(FULL, len != 0);
+        if (dense) {
+          DenseItem it;
+          it.pos = ((u64)rc.slot * a.nt + q) * (kTileCols / 2);
+          it.v = rc.v;
+          dl[__popc(dm & lt)] = it;
+        }
+        if (len != 0) {
+          SparseItem it;
+          it.s0 = s0;
+          it.v = rc.v;
+          it.kb = a.wB * rc.br + (u64)q * kTileCols;
+          it.len = len;
+          it.pad = 0;
+          sl[__popc(sm & lt)] = it;
+        }
+        __syncwarp();
+        const int nd = __popc(dm), ns = __popc(sm);
+        for (int k = 0; k < nd; k += BATCH) {
+          double2 b0[BATCH], b1[BATCH];
+          double vv[BATCH];
+#pragma unroll
+          for (int x = 0; x < BATCH; ++x) {
+            if (k + x < nd) {
+              const DenseItem it = dl[k + x];
+              vv[x] = it.v;
+              b0[x] = bd2[it.pos + lane];
+              b1[x] = bd2[it.pos + 32 + lane];
+            } else {
+              vv[x] = 0.0;
+              b0[x] = make_double2(0.0, 0.0);
+              b1[x] = b0[x];
+            }
+          }
+#pragma unroll
+          for (int x = 0; x < BATCH; ++x) {
+            acc0 = fma(vv[x], b0[x].x, acc0);
+            acc1 = fma(vv[x], b0[x].y, acc1);
+            acc2 = fma(vv[x], b1[x].x, acc2);
+            acc3 = fma(vv[x], b1[x].y, acc3);
           }
         }
-        const int n = (int)(e1 - eb < 32 ? e1 - eb : 32);
-        for (int k = 0; k < n; ++k) {
-          const double vk = __shfl_sync(FULL, v, k);
-          const int sk = __shfl_sync(FULL, slot, k);
-          if (sk >= 0) {
-            const double2 b = bd2[((u64)sk * a.nt + q) * 32 + lane];
-            acc0 = fma(vk, b.x, acc0);
-            acc1 = fma(vk, b.y, acc1);
-            continue;
+        for (int k = 0; k < ns; ++k) {
+          const SparseItem it = sl[k];
+          for (u32 x = lane; x < it.len; x += 32) {
+            const u32 j = (u32)(a.bk[it.s0 + x] - it.kb);
+            sacc[j] = fma(it.v, a.bv[it.s0 + x], sacc[j]);
           }
-          const u32 lk = __shfl_sync(FULL, len, k);
-          if (lk == 0) continue;
-          const u64 sk0 = __shfl_sync(FULL, s0, k);
-          const u64 kb = a.wB * __shfl_sync(FULL, br, k) + (u64)q * kTileCols;  // key of the tile's column 0
-          u32 jl = 64, jh = 64;
-          double wl = 0.0, wh = 0.0;
-          if ((u32)lane < lk) {
-            jl = (u32)(a.bk[sk0 + lane] - kb);
-            wl = a.bv[sk0 + lane];
-          }
-          if ((u32)lane + 32 < lk) {
-            jh = (u32)(a.bk[sk0 + 32 + lane] - kb);
-            wh = a.bv[sk0 + 32 + lane];
-          }
-          const u32 mlo = __reduce_or_sync(FULL, (jl < 32 ? 1u << jl : 0u) | (jh < 32 ? 1u << jh : 0u));
-          const u32 mhi = __reduce_or_sync(FULL, (jl >= 32 && jl < 64 ? 1u << (jl - 32) : 0u) |
-                                                     (jh >= 32 && jh < 64 ? 1u << (jh - 32) : 0u));
-          const u64 m = ((u64)mhi << 32) | mlo;
-          const int c0 = 2 * lane;
-          const bool has0 = (m >> c0) & 1ull, has1 = (m >> (c0 + 1)) & 1ull;
-          const int i0 = __popcll(m & ((1ull << c0) - 1ull));  // entry index of column c0 (if present)
-          const int i1 = i0 + (int)has0;                        // entry index of column c0 + 1
-          const double x0l = __shfl_sync(FULL, wl, i0 & 31), x0h = __shfl_sync(FULL, wh, i0 & 31);
-          const double x1l = __shfl_sync(FULL, wl, i1 & 31), x1h = __shfl_sync(FULL, wh, i1 & 31);
-          if (has0) acc0 = fma(vk, i0 < 32 ? x0l : x0h, acc0);
-          if (has1) acc1 = fma(vk, i1 < 32 ? x1l : x1h, acc1);
+          __syncwarp();
         }
+        had_sparse |= ns != 0;
+        __syncwarp();
       }
-      stage[i * kStageStride + 2 * lane] = acc0;
-      stage[i * kStageStride + 2 * lane + 1] = acc1;
+      if (had_sparse) {
+        acc0 += sacc[2 * lane];
+        acc1 += sacc[2 * lane + 1];
+        acc2 += sacc[64 + 2 * lane];
+        acc3 += sacc[65 + 2 * lane];
+        sacc[2 * lane] = 0.0;
+        sacc[2 * lane + 1] = 0.0;
+        sacc[64 + 2 * lane] = 0.0;
+        sacc[65 + 2 * lane] = 0.0;
+        __syncwarp();
+      }
+      double* st = stage + i * kStageStride;
+      st[2 * lane] = acc0;
+      st[2 * lane + 1] = acc1;
+      st[64 + 2 * lane] = acc2;
+      st[65 + 2 * lane] = acc3;
     }
     __syncthreads();
-    for (int jj = warp; jj < kTileCols; jj += kTileThreads / 32) {
+    for (int jj = warp; jj < kTileCols; jj += kTileWarps) {
       const u64 col = (u64)q * kTileCols + jj;
       if (col >= a.wB) continue;
       unsigned long long pos = a.base[(t * a.wB + col) * a.np + p];
@@ -336,10 +439,10 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
 #pragma unroll
       for (int g = 0; g < kPanelRows / 32; ++g) {
         const int i = g * 32 + lane;
-        const bool bit = (s_bits[i] >> jj) & 1ull;
+        const bool bit = (s_bits[i][jj >> 6] >> (jj & 63)) & 1ull;
         const u32 m = __ballot_sync(FULL, bit);
         if (bit) {
-          const u64 o = pos + __popc(m & ((1u << lane) - 1u));
+          const u64 o = pos + __popc(m & lt);
           a.ck[o] = keybase + i;
           a.cv[o] = stage[i * kStageStride + jj];
         }
@@ -359,10 +462,10 @@ int grid_cap(u64 work, int threads, int per_sm = 8) {
 }  // namespace
 
 bool tile_shape_ok(u64 h, u64 w, u64 wB, u64 d, u64 na, u64 nb) {
-  if (na >= (1ull << 32) || nb >= (1ull << 32)) return false;
+  if (na >= (1ull << 32) || nb >= (1ull << 32) || w * d >= (1ull << 31)) return false;
   const TileDims t = tile_dims(h, w, wB, d, nb);
-  const unsigned __int128 cb = (unsigned __int128)h * d * t.nt * 8;
-  const unsigned __int128 bb = (unsigned __int128)w * d * (t.nt + 1) * 12;
+  const unsigned __int128 cb = (unsigned __int128)h * d * t.nw * 8;
+  const unsigned __int128 bb = (unsigned __int128)w * d * (t.nt + 1 + t.nw) * 8;
   const unsigned __int128 cn = (unsigned __int128)d * wB * t.np * 12;
   return cb <= kMaxBitmapBytes && bb <= kMaxBitmapBytes && cn <= kMaxBitmapBytes;
 }
@@ -388,7 +491,8 @@ int run_tile_mult(const u64* akeys, const double* avals, u64 na, const u64* bkey
   u64* arow = (u64*)at(L.arow);
   u64* brow = (u64*)at(L.brow);
   int* dslot = (int*)at(L.dslot);
-  u32* tp = (u32*)at(L.tp);
+  u64* tp = (u64*)at(L.tp);
+  ARec* rec = (ARec*)at(L.arec);
   u64* bbits = (u64*)at(L.bbits);
   double* bd = (double*)at(L.bd);
   u64* cbits = (u64*)at(L.cbits);
@@ -427,40 +531,42 @@ int run_tile_mult(const u64* akeys, const double* avals, u64 na, const u64* bkey
     tile_rowptr_kernel<<<grid_cap(nb + 1, 256), 256, 0, s>>>(bk, nb, d_nb, make_divider(wB), brows, brow);
     count_launch(2);
   }
-  if (cudaMemsetAsync(tp, 0, brows * (u64)(t.nt + 1) * 4, s) != cudaSuccess) return LNT_DEVICE_ERROR;
-  if (cudaMemsetAsync(bbits, 0, brows * (u64)t.nt * 8, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  if (cudaMemsetAsync(bbits, 0, brows * (u64)t.nw * 8, s) != cudaSuccess) return LNT_DEVICE_ERROR;
   if (t.smax && cudaMemsetAsync(bd, 0, t.smax * (u64)t.nt * kTileCols * 8, s) != cudaSuccess)
     return LNT_DEVICE_ERROR;
   {
     ProfScope prof("tile_bprep", s);
     tile_slot_kernel<<<grid_cap(brows, 256), 256, 0, s>>>(brow, brows, std::max<u64>(wB, kTileCols), t.smax, dslot,
                                                          slot_counter);
-    tile_bentry_kernel<<<grid_cap(nb, 256), 256, 0, s>>>(bk, bv, d_nb, brow, make_divider(wB), wB, t.nt, dslot,
-                                                        bbits, tp, bd);
-    count_launch(2);
+    tile_bentry_kernel<<<grid_cap(nb, 256), 256, 0, s>>>(bk, bv, d_nb, brow, make_divider(wB), wB, t.nt, t.nw,
+                                                        dslot, bbits, tp, bd);
+    tile_tp_empty_kernel<<<grid_cap(brows, 256), 256, 0, s>>>(brow, brows, t.nt, tp);
+    tile_arec_kernel<<<grid_cap(na, 256), 256, 0, s>>>(ak, av, na, w, make_divider(w), make_divider(h), dslot, rec);
+    count_launch(4);
   }
   {
     ProfScope prof("tile_cbits", s);
-    tile_cbits_kernel<<<grid_cap(crows * 32, 256), 256, 0, s>>>(ak, arow, bbits, h, w, d, t.nt, make_divider(h),
+    tile_cbits_kernel<<<grid_cap(crows * 32, 256), 256, 0, s>>>(ak, arow, bbits, h, w, d, t.nw, make_divider(h),
                                                                cbits);
     count_launch();
   }
   {
     ProfScope prof("tile_count", s);
-    tile_count_kernel<<<grid_cap(d * t.np * (u64)t.nt * 32, 256), 256, 0, s>>>(cbits, h, wB, d, t.nt, t.np, cnt);
+    tile_count_kernel<<<grid_cap(d * t.np * (u64)t.nw * 32, 256), 256, 0, s>>>(cbits, h, wB, d, t.nw, t.np, cnt);
     count_launch();
   }
   if ((st = scan::run(CountGet{cnt}, ncnt, base, (unsigned long long*)d_nc, at(L.scan), s, "tile_scan")) != LNT_OK)
     return st;
-  NumArgs a{ak, av, arow, bk, bv, brow, dslot, tp, bd, cbits, base, h, w, wB, d, t.nt, t.np,
-            d * (u64)t.np * t.nt, ck, cv};
+  NumArgs a{rec, arow, bk, bv, tp, bd, cbits, base, h, w, wB, d, t.nt, t.nw, t.np, d * (u64)t.np * t.nt, ck, cv};
   {
     ProfScope prof("tile_numeric", s);
-    if (cudaFuncSetAttribute(tile_numeric_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes) !=
-        cudaSuccess)
+    const char* eb = std::getenv("LNT_TILE_BATCH");
+    const bool b4 = eb && std::atoi(eb) == 4;
+    auto kern = b4 ? tile_numeric_kernel<4> : tile_numeric_kernel<kDenseBatch>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNumericSmem) != cudaSuccess)
       return LNT_DEVICE_ERROR;
     const u64 grid = std::min<u64>(a.units, (u64)sm_count() * 2);
-    tile_numeric_kernel<<<(unsigned)std::max<u64>(grid, 1), kTileThreads, kStageBytes, s>>>(a);
+    kern<<<(unsigned)std::max<u64>(grid, 1), kTileThreads, kNumericSmem, s>>>(a);
     count_launch();
   }
   return launch_status();
