@@ -11,27 +11,27 @@
 //   B row-major: B re-keyed to j + wB*(c + w*t), sorted, duplicate keys
 //     summed, with row pointers (w*d + 1); a row holding at least a quarter of
 //     its columns is also expanded into a dense row of Bd (one slot per such
-//     row, zero-filled, padded to whole 128-column tiles); for every row
+//     row, zero-filled, padded to whole 256-column tiles); for every row
 //     tp[row][q] = position in B of the row's first entry at or right of
-//     column 128q (q = 0..nt);
+//     column 256q (q = 0..nt);
 //   A records: per A entry its B row (c + w*t), that row's dense slot and the
 //     value, 16 bytes, so one load per entry serves every tile;
 //   bitmaps, one bit per (row, column), 64-column words: Bbits (B rows) and
 //     Cbits (C rows, = OR of the Bbits rows that A row selects) — the output
 //     pattern, computed before any arithmetic.
-// Output positions: per (tab, column, panel of 64 rows) the number of
+// Output positions: per (tab, column, panel of 32 rows) the number of
 // pattern bits, exclusive-scanned in (tab, column, panel) order, so each
 // panel's rows of one column land at a known contiguous offset.
-// Numeric pass: one CTA per (panel, 128-column tile) unit; warps take rows
-// from a shared counter, four columns per lane in registers.  Each 32-entry
+// Numeric pass: one CTA per (panel, 256-column tile) unit; warps take rows
+// from a shared counter, eight columns per lane in registers.  Each 32-entry
 // chunk of the row's A records is split by ballot into per-warp shared lists
 // of dense-row items (Bd position, value) and sparse-row items (segment,
 // value), so the inner loops read one broadcast shared-memory item per entry:
-// a dense item adds two coalesced 512-byte loads and four FMAs (several items'
-// loads issued before their FMAs), a sparse item's segment is scattered by
-// the lanes into a per-warp shared accumulator row (distinct columns within
-// a segment).  The 64 x 128 tile is staged in shared memory and written
-// column by column (contiguous runs).
+// a dense item adds four coalesced 512-byte loads and eight FMAs, a sparse
+// item's segment is scattered by the lanes into the row's staging row in
+// shared memory (distinct columns within a segment).  The 32 x 256 tile is
+// staged in shared memory and written column by column (contiguous runs),
+// at offsets fetched before the unit's arithmetic.
 #include <algorithm>
 #include <cstdlib>
 
@@ -48,13 +48,13 @@ namespace {
 
 constexpr u32 FULL = 0xffffffffu;
 constexpr int kWordCols = 64;      // columns per bitmap word
-constexpr int kTileCols = 128;     // output columns per numeric tile (four per lane)
-constexpr int kPanelRows = 64;     // output rows per unit
+constexpr int kTileCols = 256;     // output columns per numeric tile (eight per lane)
+constexpr int kPanelRows = 32;     // output rows per unit
 constexpr int kTileThreads = 512;  // 16 warps
 constexpr int kTileWarps = kTileThreads / 32;
-constexpr int kTileGroup = 8;      // tiles of one panel processed by consecutive units
-constexpr int kStageStride = 129;  // doubles per staged row
-constexpr int kDenseBatch = 2;     // dense items whose loads are issued before their FMAs (LNT_TILE_BATCH=4: four)
+constexpr int kTileGroup = 4;      // tiles of one panel processed by consecutive units
+constexpr int kStageStride = 257;  // doubles per staged row
+constexpr int kSparseBatch = 4;    // sparse segments whose first 32 entries are loaded together
 
 struct ARec {
   u32 br;    // B row c + w*t
@@ -73,13 +73,12 @@ struct SparseItem {
   u32 pad;
 };
 constexpr size_t kStageBytes = (size_t)kPanelRows * kStageStride * 8;
-constexpr size_t kNumericSmem = kStageBytes + (size_t)kTileWarps * 32 * (sizeof(DenseItem) + sizeof(SparseItem)) +
-                                (size_t)kTileWarps * kTileCols * 8;
+constexpr size_t kNumericSmem = kStageBytes + (size_t)kTileWarps * 32 * (sizeof(DenseItem) + sizeof(SparseItem));
 constexpr size_t kMaxBitmapBytes = 16ull << 30;
 
 struct TileDims {
   u64 h, w, wB, d;
-  u32 nt, nw, np;  // 128-column tiles per row, 64-column bitmap words per row, 64-row panels per tab
+  u32 nt, nw, np;  // 256-column tiles per row, 64-column bitmap words per row, 32-row panels per tab
   u64 smax;    // dense-row slots
 };
 
@@ -301,20 +300,18 @@ struct NumArgs {
   double* cv;
 };
 
-template <int BATCH>
 __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   double* stage = reinterpret_cast<double*>(smem);  // [kPanelRows][kStageStride]
   DenseItem* dlist = reinterpret_cast<DenseItem*>(smem + kStageBytes);
   SparseItem* slist = reinterpret_cast<SparseItem*>(dlist + kTileWarps * 32);
-  double* sacc_all = reinterpret_cast<double*>(slist + kTileWarps * 32);
-  __shared__ u64 s_bits[kPanelRows][2];
+  constexpr int kWords = kTileCols / kWordCols;
+  __shared__ u64 s_bits[kPanelRows][kWords];
+  __shared__ unsigned long long s_base[kTileCols];
   __shared__ u32 s_next;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   DenseItem* dl = dlist + warp * 32;
   SparseItem* sl = slist + warp * 32;
-  double* sacc = sacc_all + warp * kTileCols;
-  for (int c = lane; c < kTileCols; c += 32) sacc[c] = 0.0;
   const u32 lt = (1u << lane) - 1u;
   const double2* bd2 = reinterpret_cast<const double2*>(a.bd);
   const u64 per_tab = (u64)a.np * a.nt;
@@ -327,10 +324,15 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
     const u32 p = (u32)(within / gs);
     const u32 q = (u32)(qg * kTileGroup + (within - (u64)p * gs));
     const u64 row0 = (u64)p * kPanelRows;
-    if (threadIdx.x < 2 * kPanelRows) {
-      const u64 r = row0 + (threadIdx.x >> 1);
-      const u32 word = 2 * q + (threadIdx.x & 1);
-      s_bits[threadIdx.x >> 1][threadIdx.x & 1] = r < a.h && word < a.nw ? a.cbits[(r + a.h * t) * a.nw + word] : 0ull;
+    if (threadIdx.x < kPanelRows * kWords) {
+      const int i = threadIdx.x / kWords, wd = threadIdx.x % kWords;
+      const u64 r = row0 + i;
+      const u32 word = kWords * q + wd;
+      s_bits[i][wd] = r < a.h && word < a.nw ? a.cbits[(r + a.h * t) * a.nw + word] : 0ull;
+    }
+    if (threadIdx.x < kTileCols) {
+      const u64 col = (u64)q * kTileCols + threadIdx.x;
+      s_base[threadIdx.x] = col < a.wB ? a.base[(t * a.wB + col) * a.np + p] : 0ull;
     }
     if (threadIdx.x == 0) s_next = 0;
     __syncthreads();
@@ -339,10 +341,16 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
       if (lane == 0) i = atomicAdd(&s_next, 1u);
       i = __shfl_sync(FULL, i, 0);
       if (i >= (u32)kPanelRows) break;
-      if ((s_bits[i][0] | s_bits[i][1]) == 0ull) continue;
+      u64 any = 0;
+#pragma unroll
+      for (int wd = 0; wd < kWords; ++wd) any |= s_bits[i][wd];
+      if (any == 0ull) continue;
       const u64 row = row0 + i + a.h * t;
       const u64 e0 = a.arow[row], e1 = a.arow[row + 1];
-      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+      double* st = stage + i * kStageStride;
+      double acc[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = 0.0;
       bool had_sparse = false;
       for (u64 eb = e0; eb < e1; eb += 32) {
         const u64 e = eb + lane;
@@ -376,77 +384,76 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
           it.pad = 0;
           sl[__popc(sm & lt)] = it;
         }
+        if (sm != 0u && !had_sparse) {  // the staging row accumulates the sparse products
+          for (int c = lane; c < kTileCols; c += 32) st[c] = 0.0;
+          had_sparse = true;
+        }
         __syncwarp();
         const int nd = __popc(dm), ns = __popc(sm);
-        for (int k = 0; k < nd; k += BATCH) {
-          double2 b0[BATCH], b1[BATCH];
-          double vv[BATCH];
+        for (int k = 0; k < nd; ++k) {
+          const DenseItem it = dl[k];
+          double2 b[4];
 #pragma unroll
-          for (int x = 0; x < BATCH; ++x) {
-            if (k + x < nd) {
-              const DenseItem it = dl[k + x];
-              vv[x] = it.v;
-              b0[x] = bd2[it.pos + lane];
-              b1[x] = bd2[it.pos + 32 + lane];
-            } else {
-              vv[x] = 0.0;
-              b0[x] = make_double2(0.0, 0.0);
-              b1[x] = b0[x];
+          for (int x = 0; x < 4; ++x) b[x] = bd2[it.pos + 32 * x + lane];
+#pragma unroll
+          for (int x = 0; x < 4; ++x) {
+            acc[2 * x] = fma(it.v, b[x].x, acc[2 * x]);
+            acc[2 * x + 1] = fma(it.v, b[x].y, acc[2 * x + 1]);
+          }
+        }
+        for (int k = 0; k < ns; k += kSparseBatch) {
+          // first 32 entries of kSparseBatch segments loaded together, then scattered one segment at a time
+          u32 jj[kSparseBatch];
+          double ww[kSparseBatch];
+#pragma unroll
+          for (int x = 0; x < kSparseBatch; ++x) {
+            jj[x] = kTileCols;
+            ww[x] = 0.0;
+            if (k + x < ns) {
+              const SparseItem it = sl[k + x];
+              if ((u32)lane < it.len) {
+                jj[x] = (u32)(a.bk[it.s0 + lane] - it.kb);
+                ww[x] = a.bv[it.s0 + lane];
+              }
             }
           }
 #pragma unroll
-          for (int x = 0; x < BATCH; ++x) {
-            acc0 = fma(vv[x], b0[x].x, acc0);
-            acc1 = fma(vv[x], b0[x].y, acc1);
-            acc2 = fma(vv[x], b1[x].x, acc2);
-            acc3 = fma(vv[x], b1[x].y, acc3);
+          for (int x = 0; x < kSparseBatch; ++x) {
+            if (k + x < ns) {
+              const SparseItem it = sl[k + x];
+              if (jj[x] < (u32)kTileCols) st[jj[x]] = fma(it.v, ww[x], st[jj[x]]);
+              for (u32 y = lane + 32; y < it.len; y += 32) {
+                const u32 j = (u32)(a.bk[it.s0 + y] - it.kb);
+                st[j] = fma(it.v, a.bv[it.s0 + y], st[j]);
+              }
+              __syncwarp();
+            }
           }
         }
-        for (int k = 0; k < ns; ++k) {
-          const SparseItem it = sl[k];
-          for (u32 x = lane; x < it.len; x += 32) {
-            const u32 j = (u32)(a.bk[it.s0 + x] - it.kb);
-            sacc[j] = fma(it.v, a.bv[it.s0 + x], sacc[j]);
-          }
-          __syncwarp();
+        __syncwarp();
+      }
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        const int c = 64 * x + 2 * lane;
+        if (had_sparse) {
+          st[c] += acc[2 * x];
+          st[c + 1] += acc[2 * x + 1];
+        } else {
+          st[c] = acc[2 * x];
+          st[c + 1] = acc[2 * x + 1];
         }
-        had_sparse |= ns != 0;
-        __syncwarp();
       }
-      if (had_sparse) {
-        acc0 += sacc[2 * lane];
-        acc1 += sacc[2 * lane + 1];
-        acc2 += sacc[64 + 2 * lane];
-        acc3 += sacc[65 + 2 * lane];
-        sacc[2 * lane] = 0.0;
-        sacc[2 * lane + 1] = 0.0;
-        sacc[64 + 2 * lane] = 0.0;
-        sacc[65 + 2 * lane] = 0.0;
-        __syncwarp();
-      }
-      double* st = stage + i * kStageStride;
-      st[2 * lane] = acc0;
-      st[2 * lane + 1] = acc1;
-      st[64 + 2 * lane] = acc2;
-      st[65 + 2 * lane] = acc3;
     }
     __syncthreads();
     for (int jj = warp; jj < kTileCols; jj += kTileWarps) {
       const u64 col = (u64)q * kTileCols + jj;
       if (col >= a.wB) continue;
-      unsigned long long pos = a.base[(t * a.wB + col) * a.np + p];
-      const u64 keybase = a.h * (col + a.wB * t) + row0;
-#pragma unroll
-      for (int g = 0; g < kPanelRows / 32; ++g) {
-        const int i = g * 32 + lane;
-        const bool bit = (s_bits[i][jj >> 6] >> (jj & 63)) & 1ull;
-        const u32 m = __ballot_sync(FULL, bit);
-        if (bit) {
-          const u64 o = pos + __popc(m & lt);
-          a.ck[o] = keybase + i;
-          a.cv[o] = stage[i * kStageStride + jj];
-        }
-        pos += __popc(m);
+      const bool bit = (s_bits[lane][jj >> 6] >> (jj & 63)) & 1ull;
+      const u32 m = __ballot_sync(FULL, bit);
+      if (bit) {
+        const u64 o = s_base[jj] + __popc(m & lt);
+        a.ck[o] = a.h * (col + a.wB * t) + row0 + lane;
+        a.cv[o] = stage[lane * kStageStride + jj];
       }
     }
     __syncthreads();
@@ -560,9 +567,7 @@ int run_tile_mult(const u64* akeys, const double* avals, u64 na, const u64* bkey
   NumArgs a{rec, arow, bk, bv, tp, bd, cbits, base, h, w, wB, d, t.nt, t.nw, t.np, d * (u64)t.np * t.nt, ck, cv};
   {
     ProfScope prof("tile_numeric", s);
-    const char* eb = std::getenv("LNT_TILE_BATCH");
-    const bool b4 = eb && std::atoi(eb) == 4;
-    auto kern = b4 ? tile_numeric_kernel<4> : tile_numeric_kernel<kDenseBatch>;
+    auto kern = tile_numeric_kernel;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNumericSmem) != cudaSuccess)
       return LNT_DEVICE_ERROR;
     const u64 grid = std::min<u64>(a.units, (u64)sm_count() * 2);
