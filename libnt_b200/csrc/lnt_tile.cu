@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
   __shared__ u64 s_bits[kPanelRows][kWords];
   __shared__ unsigned long long s_base[kTileCols];
   __shared__ u32 s_next;
+  __shared__ u64 s_unit[4];  // first C row (row0 + h*t), first column + wB*t, tile q, row0
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   DenseItem* dl = dlist + warp * 32;
   SparseItem* sl = slist + warp * 32;
@@ -334,7 +335,13 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
       const u64 col = (u64)q * kTileCols + threadIdx.x;
       s_base[threadIdx.x] = col < a.wB ? a.base[(t * a.wB + col) * a.np + p] : 0ull;
     }
-    if (threadIdx.x == 0) s_next = 0;
+    if (threadIdx.x == 0) {
+      s_next = 0;
+      s_unit[0] = row0 + a.h * t;
+      s_unit[1] = (u64)q * kTileCols + a.wB * t;
+      s_unit[2] = q;
+      s_unit[3] = row0;
+    }
     __syncthreads();
     for (;;) {
       u32 i = 0;
@@ -345,7 +352,8 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
 #pragma unroll
       for (int wd = 0; wd < kWords; ++wd) any |= s_bits[i][wd];
       if (any == 0ull) continue;
-      const u64 row = row0 + i + a.h * t;
+      const u64 row = s_unit[0] + i;
+      const u32 q = (u32)s_unit[2];
       const u64 e0 = a.arow[row], e1 = a.arow[row + 1];
       double* st = stage + i * kStageStride;
       double acc[8];
@@ -446,13 +454,12 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_numeric_kernel(NumArgs a
     }
     __syncthreads();
     for (int jj = warp; jj < kTileCols; jj += kTileWarps) {
-      const u64 col = (u64)q * kTileCols + jj;
-      if (col >= a.wB) continue;
+      if ((u64)s_unit[2] * kTileCols + jj >= a.wB) continue;
       const bool bit = (s_bits[lane][jj >> 6] >> (jj & 63)) & 1ull;
       const u32 m = __ballot_sync(FULL, bit);
       if (bit) {
         const u64 o = s_base[jj] + __popc(m & lt);
-        a.ck[o] = a.h * (col + a.wB * t) + row0 + lane;
+        a.ck[o] = a.h * (s_unit[1] + jj) + s_unit[3] + lane;
         a.cv[o] = stage[lane * kStageStride + jj];
       }
     }
