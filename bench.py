@@ -52,14 +52,14 @@ def peaks():
     return HBM_FALLBACK_GBS, "fallback"
 
 
-def profile_traffic(name: str):
-    """Per-pair DRAM traffic of a kernel from the committed ncu summary
-    (line 'traffic_bytes_per_pair: X'), or None."""
+def profile_traffic(name: str, key: str = "traffic_bytes_per_pair"):
+    """Per-unit DRAM traffic of a kernel from the committed ncu summary
+    (line '<key>: X'), or None."""
     f = ROOT / "profiles" / f"{name}.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_pair:"):
+        if line.strip().startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -354,8 +354,8 @@ def run_ours(args):
     avg_ms = os_ms / max(os_launches, 1)
     alg_bytes = 32.0 * n  # read 16 B + write 16 B per pair per pass
     achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
-    tpp = profile_traffic("sort_onesweep_merge_512x4_2x64M")
-    roofline = {"bound": "hbm", "kernel": "sort_onesweep (one 9-bit LSD digit pass over 2^27 (u64,f64) pairs)",
+    tpp = profile_traffic("onesweep8_bucket_merge_512x4_2x64M")
+    roofline = {"bound": "hbm", "kernel": "sort_onesweep (one 8-bit digit pass of the bucketed sort over 2^27 (u64,f64) pairs)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
@@ -869,6 +869,7 @@ def run_skewed(args):
     peak, peak_kind = peaks()
     alg = 16.0 * (ak.numel() + bk.numel() + n_out)
     num_ms = kernels["tile_numeric"]
+    tpo = profile_traffic("tile_numeric_skewed_2x32M", "traffic_bytes_per_output")
     cpu = None
     if not args.no_cpu and world == 1:
         import oracle
@@ -896,7 +897,9 @@ def run_skewed(args):
                      "achieved": alg / (num_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (num_ms * 1e-3) / 1e9 / peak, "alg_bytes_per_launch": alg,
                      "avg_launch_ms": num_ms, "peak_source": peak_kind,
-                     "step_frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None},
+                     "step_frac": alg / (ms * 1e-3) / 1e9 / peak,
+                     "traffic": (tpo * n_out) if tpo else None,
+                     "traffic_note": "DRAM bytes per output entry from the small-case ncu capture, times the output count"},
         "cpu_baseline": cpu, "clocks": sampler.summary(),
     })), flush=True)
     return 0
