@@ -284,9 +284,9 @@ LNT_API int lnt_dense_lattice_mult_split(const double* A, const double* B, doubl
  * B (power-of-two scaled), products computed exactly modulo `moduli` pairwise
  * coprime integers <= 256 as INT8 tensor-core GEMMs with INT32 accumulation,
  * and reconstructed by Chinese remaindering in double-double;
- * beta = floor((log2 prod(moduli) - log2 w - 3) / 2), error about
- * 2^(2-beta) |A||B| per entry (13 moduli: beta = 43 at w = 16384; 16 moduli:
- * beta = 55).  Requires w < 2^17 and 2 <= moduli <= 20. */
+ * beta = min(floor((log2 prod(moduli) - log2 w - 3) / 2), 53), error about
+ * 2^(2-beta) |A||B| per entry (13 moduli: beta = 42 at w = 16384; 16 moduli:
+ * beta = 53).  Requires w < 2^17 and 2 <= moduli <= 20. */
 LNT_API int lnt_dense_crt_workspace(int64_t h, int64_t w, int64_t wB, int moduli, size_t* bytes);
 LNT_API int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int64_t h,
                                        int64_t w, int64_t wB, int64_t d, int moduli,

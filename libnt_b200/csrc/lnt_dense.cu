@@ -277,6 +277,7 @@ int lt_dgemm(const double* A, const double* B, double* C, u64 m, u64 n, u64 k, v
 // componentwise; N moduli give beta = floor((log2 M - log2 K - 3) / 2).
 // ===========================================================================
 constexpr int kMaxModuli = 20;
+constexpr int kMaxLimbs = 6;  // 6 x 27 bits > log2 of the product of 20 moduli
 // pairwise coprime, all <= 256 so symmetric residues fit in int8
 constexpr int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                                      223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
@@ -285,12 +286,20 @@ struct CrtParams {
   int n;        // moduli used
   int beta;     // integer bits of A' and B'
   int m[kMaxModuli];
+  double md[kMaxModuli];        // m_l as a double
   int u[kMaxModuli];            // (M/m_l)^-1 mod m_l
   double rinv_hi[kMaxModuli];   // 1/m_l as a double-double
   double rinv_lo[kMaxModuli];
   float rinv_f[kMaxModuli];     // 1/m_l in float
   double M_hi, M_lo;            // M as a double-double
+  // exact remaindering: X = sum_l p_l V_l (mod M), V_l = (M/m_l) u_l < M, in
+  // kLimbBits-bit limbs; M in the same limbs; 1/M for the quotient estimate
+  int lv;                       // limbs of M
+  u32 V[kMaxModuli][kMaxLimbs];
+  u32 Ml[kMaxLimbs];
+  double Minv;
 };
+constexpr int kLimbBits = 27;  // n * 2^31 * 2^27 < 2^63 for n <= 20 moduli
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
   s = a + b;
@@ -330,11 +339,19 @@ __device__ __forceinline__ double scale2(double x, int e) {
   return (x * pow2(e1)) * pow2(e - e1);
 }
 
-__device__ __forceinline__ signed char sym_res(double x, int l, const CrtParams& P) {
-  const double m = (double)P.m[l];
-  double r = dmod(x, m, P.rinv_hi[l]);
-  if (r >= (double)((P.m[l] + 1) / 2)) r -= m;
-  return (signed char)(int)r;
+// A residue of the integer-valued double x (|x| < 2^56) modulo m_l in
+// [-128, 127]: q = x / m rounded to nearest by adding 1.5 * 2^52 (exact
+// integer spacing), r = x - q m exact by fma, |r| <= m/2 + 1 (q may be one off
+// next to a half); the low word of r + 1.5 * 2^52 is r as an int.  Any
+// representative congruent modulo m serves the modular products.
+__device__ __forceinline__ int sym_res(double x, int l, const CrtParams& P) {
+  constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+  const double q = fma(x, P.rinv_hi[l], kRound) - kRound;
+  const double r = fma(-q, P.md[l], x);
+  int ri = __double2loint(r + kRound);
+  if (ri > 127) ri -= P.m[l];
+  if (ri < -128) ri += P.m[l];
+  return ri;
 }
 
 // Per-row maximum exponent of A (col-major) over a chunk of columns; eA must
@@ -358,9 +375,18 @@ __global__ void fill_int_kernel(int* __restrict__ p, u64 n, int v) {
   if (i < n) p[i] = v;
 }
 
+// Four residues (of four consecutive K entries) packed into one 32-bit word.
+__device__ __forceinline__ u32 pack_res4(const double (&x)[4], int l, const CrtParams& P) {
+  u32 v = 0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) v |= ((u32)sym_res(x[c], l, P) & 0xffu) << (8 * c);
+  return v;
+}
+
 // A (h x w col-major) -> residues res[l]: Mp rows of Kp int8 (row-major, K
 // contiguous).  Tile of 32 rows x 128 columns through shared memory: read
-// along rows (coalesced), write along K (each warp stores 32 consecutive bytes).
+// along rows (coalesced); each lane then turns four consecutive K entries of a
+// row into one 4-byte word per modulus (a warp stores 128 consecutive bytes).
 __global__ void __launch_bounds__(256) residue_a_kernel(const double* __restrict__ A, u64 h, u64 w, u64 Mp, u64 Kp,
                                                         const int* __restrict__ eA, CrtParams P,
                                                         signed char* __restrict__ res) {
@@ -372,64 +398,95 @@ __global__ void __launch_bounds__(256) residue_a_kernel(const double* __restrict
     tile[lane][kk] = (i < h && k < w) ? A[i + h * k] : 0.0;
   }
   __syncthreads();
+  const u64 k = k0 + 4 * lane;  // Kp is a multiple of 16, so k < Kp keeps all four in the row
+  if (k >= Kp) return;
   for (int rr = warp; rr < 32; rr += 8) {
     const u64 i = i0 + rr;
     if (i >= h) continue;
     const int sc = P.beta - eA[i];
+    double x[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const u64 k = k0 + q * 32 + lane;
-      if (k >= Kp) continue;
-      const double x = rint(scale2(tile[rr][q * 32 + lane], sc));
-      signed char* dst = res + i * Kp + k;
-      for (int l = 0; l < P.n; ++l) dst[(u64)l * Mp * Kp] = sym_res(x, l, P);
-    }
+    for (int c = 0; c < 4; ++c) x[c] = rint(scale2(tile[rr][4 * lane + c], sc));
+    u32* dst = reinterpret_cast<u32*>(res + i * Kp + k);
+    const u64 plane = Mp * Kp / 4;
+    for (int l = 0; l < P.n; ++l) dst[(u64)l * plane] = pack_res4(x, l, P);
   }
 }
 
 // B (w x wB col-major) -> residues res[l]: Np rows (columns of B) of Kp int8.
+// Grid: y over columns of B, x over groups of four K entries (one 4-byte word
+// per modulus; entries beyond w are zero).
 __global__ void residue_b_kernel(const double* __restrict__ B, u64 w, u64 wB, u64 Np, u64 Kp,
                                  const int* __restrict__ eB, CrtParams P, signed char* __restrict__ res) {
-  const u64 total = w * wB;
-  const u64 stride = (u64)gridDim.x * blockDim.x;
-  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
-    const u64 j = t / w, k = t - j * w;
-    const double x = rint(scale2(B[t], P.beta - eB[j]));
-    signed char* dst = res + j * Kp + k;
-    for (int l = 0; l < P.n; ++l) dst[(u64)l * Np * Kp] = sym_res(x, l, P);
+  const u64 plane = Np * Kp / 4;
+  for (u64 j = blockIdx.y; j < wB; j += gridDim.y) {
+    const int sc = P.beta - eB[j];
+    const double* col = B + w * j;
+    u32* dst = reinterpret_cast<u32*>(res + j * Kp);
+    for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; 4 * g < Kp; g += (u64)gridDim.x * blockDim.x) {
+      double x[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) x[c] = 4 * g + c < w ? rint(scale2(col[4 * g + c], sc)) : 0.0;
+      for (int l = 0; l < P.n; ++l) dst[(u64)l * plane + g] = pack_res4(x, l, P);
+    }
   }
 }
 
-// Chinese remaindering of the P.n INT32 products, scaled back to float64.
-// Grid: x over rows of C (coalesced), y over columns.
-__global__ void crt_kernel(const int* __restrict__ prod, u64 Mp, u64 Np, u64 h, u64 wB, CrtParams P,
-                           const int* __restrict__ eA, const int* __restrict__ eB, double* __restrict__ C) {
+// Chinese remaindering of the P.n INT32 products, exact in integers, scaled
+// back to float64.  Per entry: T = sum_l p_l V_l as LV+1 signed 64-bit limb
+// sums (27-bit limbs; |p_l| < 2^31 so each sum stays below 2^63), carried into
+// normalised limbs; q = round(T / M) from a double estimate, exact because
+// A'B' = T - q M satisfies |A'B'| <= M/32 (the choice of beta) while the
+// estimate errs by under 2^-15; X = T - q M in limbs, converted to double
+// once (Horner from the top limb).  Grid: x over rows of C (coalesced), y over
+// columns.
+template <int LV>
+__global__ void __launch_bounds__(256) crt_kernel(const int* __restrict__ prod, u64 Mp, u64 Np, u64 h, u64 wB,
+                                                  CrtParams P, const int* __restrict__ eA,
+                                                  const int* __restrict__ eB, double* __restrict__ C) {
   const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= h) return;
   const u64 plane = Mp * Np;
   const int ea = eA[i] - 2 * P.beta;
+  constexpr long long kMask = (1ll << kLimbBits) - 1;
+  constexpr double kRadix = (double)(1ll << kLimbBits);
   for (u64 j = blockIdx.y; j < wB; j += gridDim.y) {
     const u64 src = i + Mp * j;
-    double sh = 0.0, sl = 0.0;  // S as a double-double
+    long long acc[LV + 1];
+#pragma unroll
+    for (int b = 0; b <= LV; ++b) acc[b] = 0;
 #pragma unroll 4
     for (int l = 0; l < P.n; ++l) {
-      const double m = (double)P.m[l];
-      const double r = dmod((double)__ldcs(prod + (u64)l * plane + src), m, P.rinv_hi[l]);
-      const float y = fmod_small((float)r * (float)P.u[l], (float)P.m[l], P.rinv_f[l]);
-      const double yd = (double)y;
-      const double ph = yd * P.rinv_hi[l];
-      const double pl = fma(yd, P.rinv_hi[l], -ph) + yd * P.rinv_lo[l];  // y/m_l = ph + pl
-      double s, e;
-      two_sum(sh, ph, s, e);
-      e += sl + pl;
-      two_sum(s, e, sh, sl);
+      const int pl = __ldcs(prod + (u64)l * plane + src);
+#pragma unroll
+      for (int b = 0; b < LV; ++b) acc[b] += (long long)pl * (int)P.V[l][b];  // 32 x 32 -> 64
     }
-    const double q = rint(sh);
-    double f, fe;
-    two_sum(sh - q, sl, f, fe);  // S - round(S), |.| < 1/2
-    // A'B' = M (S - q): double-double product, rounded once
-    const double c = f * P.M_hi + (fma(f, P.M_hi, -f * P.M_hi) + fe * P.M_hi + f * P.M_lo);
-    C[i + h * j] = scale2(c, ea + eB[j]);
+#pragma unroll
+    for (int b = 0; b < LV; ++b) {  // normalise: limbs in [0, 2^27), the top one signed
+      const long long c = acc[b] >> kLimbBits;
+      acc[b] &= kMask;
+      acc[b + 1] += c;
+    }
+    double td = (double)acc[LV];
+#pragma unroll
+    for (int b = LV - 1; b >= 0; --b) td = fma(td, kRadix, (double)acc[b]);
+    const long long q = __double2ll_rn(td * P.Minv);
+    const int qlo = (int)(q & kMask), qhi = (int)(q >> kLimbBits);  // |q| < 2^36
+#pragma unroll
+    for (int b = 0; b < LV; ++b) {
+      acc[b] -= (long long)qlo * (int)P.Ml[b];
+      acc[b + 1] -= (long long)qhi * (int)P.Ml[b];
+    }
+#pragma unroll
+    for (int b = 0; b < LV; ++b) {
+      const long long c = acc[b] >> kLimbBits;
+      acc[b] &= kMask;
+      acc[b + 1] += c;
+    }
+    double x = (double)acc[LV];
+#pragma unroll
+    for (int b = LV - 1; b >= 0; --b) x = fma(x, kRadix, (double)acc[b]);
+    C[i + h * j] = scale2(x, ea + eB[j]);
   }
 }
 
@@ -468,11 +525,12 @@ int make_crt_params(int n, u64 K, CrtParams* P) {
   double log2M = 0.0;
   for (int l = 0; l < n; ++l) {
     P->m[l] = kModuli[l];
+    P->md[l] = (double)kModuli[l];
     log2M += std::log2((double)kModuli[l]);
   }
   const int beta = (int)std::floor((log2M - std::log2((double)K) - 3.0) / 2.0);
   if (beta < 8) return LNT_UNSUPPORTED;
-  P->beta = std::min(beta, 62);
+  P->beta = std::min(beta, 53);  // |A'|, |B'| < 2^52: exact doubles, and residues by 1.5 * 2^52 rounding
   for (int l = 0; l < n; ++l) {
     const int m = P->m[l];
     long long rest = 1;  // (M / m) mod m
@@ -489,6 +547,48 @@ int make_crt_params(int n, u64 K, CrtParams* P) {
     P->rinv_hi[l] = 1.0 / m;
     P->rinv_lo[l] = std::fma(-P->rinv_hi[l], (double)m, 1.0) / m;
     P->rinv_f[l] = 1.0f / (float)m;
+  }
+  // V_l = (M / m_l) u_l and M in 27-bit limbs (little-endian), 1/M as a double
+  {
+    constexpr int NL = kMaxLimbs + 1;
+    const u64 mask = (1ull << kLimbBits) - 1;
+    u64 Mb[NL] = {1};
+    double Md = 1.0;
+    for (int l = 0; l < n; ++l) {  // M *= m_l
+      u64 carry = 0;
+      for (int b = 0; b < NL; ++b) {
+        const u64 t = Mb[b] * (u64)P->m[l] + carry;
+        Mb[b] = t & mask;
+        carry = t >> kLimbBits;
+      }
+      Md *= (double)P->m[l];
+    }
+    if (Mb[NL - 1] != 0) return LNT_UNSUPPORTED;
+    P->lv = 0;
+    for (int b = 0; b < kMaxLimbs; ++b) {
+      P->Ml[b] = (u32)Mb[b];
+      if (Mb[b]) P->lv = b + 1;
+    }
+    for (int l = 0; l < n; ++l) {
+      u64 Q[NL] = {0};  // M / m_l: long division from the top limb
+      u64 rem = 0;
+      for (int b = NL - 1; b >= 0; --b) {
+        const u64 cur = (rem << kLimbBits) | Mb[b];
+        Q[b] = cur / (u64)P->m[l];
+        rem = cur % (u64)P->m[l];
+      }
+      if (rem) return LNT_BAD_ARG;
+      u64 carry = 0;  // V_l = Q u_l < M
+      for (int b = 0; b < kMaxLimbs; ++b) {
+        const u64 t = Q[b] * (u64)P->u[l] + carry;
+        P->V[l][b] = (u32)(t & mask);
+        carry = t >> kLimbBits;
+      }
+      if (carry) return LNT_BAD_ARG;
+    }
+    for (int l = n; l < kMaxModuli; ++l)
+      for (int b = 0; b < kMaxLimbs; ++b) P->V[l][b] = 0;
+    P->Minv = 1.0 / Md;
   }
   // M as a double-double (products of small integers, exact residual by fma)
   double mh = 1.0, ml = 0.0;
@@ -632,7 +732,9 @@ int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int6
       }
       residue_a_kernel<<<dim3((unsigned)((uh + 31) / 32), (unsigned)((Kp + 127) / 128)), 256, 0, s>>>(
           At, uh, uw, L.Mp, Kp, eA, P, ra);
-      residue_b_kernel<<<sms * 16, 256, 0, s>>>(Bt, uw, uwB, L.Np, Kp, eB, P, rb);
+      const unsigned gx = (unsigned)std::min<u64>((Kp / 4 + 255) / 256, 64);
+      const unsigned gyb = (unsigned)std::min<u64>(uwB, std::max<u64>(1, (u64)sms * 64 / gx));
+      residue_b_kernel<<<dim3(gx, gyb), 256, 0, s>>>(Bt, uw, uwB, L.Np, Kp, eB, P, rb);
       count_launch(5);
     }
     for (int l = 0; l < moduli; ++l) {
@@ -644,7 +746,21 @@ int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int6
     {
       ProfScope prof("dense_crt", s);
       const unsigned gy = (unsigned)std::min<u64>(uwB, std::max<u64>(1, (u64)sms * 32 / ((uh + 255) / 256)));
-      crt_kernel<<<dim3((unsigned)((uh + 255) / 256), gy), 256, 0, s>>>(prod, L.Mp, L.Np, uh, uwB, P, eA, eB, Ct);
+      const dim3 grid((unsigned)((uh + 255) / 256), gy);
+      switch (P.lv) {
+        case 1:
+        case 2:
+        case 3:
+        case 4:
+          crt_kernel<4><<<grid, 256, 0, s>>>(prod, L.Mp, L.Np, uh, uwB, P, eA, eB, Ct);
+          break;
+        case 5:
+          crt_kernel<5><<<grid, 256, 0, s>>>(prod, L.Mp, L.Np, uh, uwB, P, eA, eB, Ct);
+          break;
+        default:
+          crt_kernel<6><<<grid, 256, 0, s>>>(prod, L.Mp, L.Np, uh, uwB, P, eA, eB, Ct);
+          break;
+      }
       count_launch();
     }
   }

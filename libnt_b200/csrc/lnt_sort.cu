@@ -469,21 +469,40 @@ int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, d
 
 namespace lnt {
 
-int run_onesweep_pass8(const PairSource& src, bool first, u64* out_k, double* out_v, u32 n, u32 shift, u32 mask,
-                       const u32* bstart, u32* status, u32* tile_counter, cudaStream_t s) {
-  using Sh = OnesweepShape<8, 256, 16>;
+namespace {
+template <int THREADS, int ITEMS, int W>
+int launch_pass8(const PairSource& src, bool first, u64* out_k, double* out_v, u32 n, u32 shift, u32 mask,
+                 const u32* bstart, u32* status, u32* tile_counter, cudaStream_t s) {
+  using Sh = OnesweepShape<8, THREADS, ITEMS>;
+  static_assert(Sh::TILE >= kOnesweepPassTile, "the look-back array is sized for kOnesweepPassTile-pair tiles");
   constexpr size_t sh = Sh::smem;
-  auto k_first = onesweep_kernel<8, 256, 16, 16, true>;
-  auto k_next = onesweep_kernel<8, 256, 16, 16, false>;
-  cudaFuncSetAttribute(first ? k_first : k_next, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  auto k = first ? onesweep_kernel<8, THREADS, ITEMS, W, true> : onesweep_kernel<8, THREADS, ITEMS, W, false>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
+    return LNT_DEVICE_ERROR;
   const u32 ntiles = (n + Sh::TILE - 1) / Sh::TILE;
   ProfScope prof("sort_onesweep", s);
-  if (first)
-    k_first<<<ntiles, 256, sh, s>>>(src, out_k, out_v, n, shift, mask, bstart, status, tile_counter);
-  else
-    k_next<<<ntiles, 256, sh, s>>>(src, out_k, out_v, n, shift, mask, bstart, status, tile_counter);
+  k<<<ntiles, THREADS, sh, s>>>(src, out_k, out_v, n, shift, mask, bstart, status, tile_counter);
   count_launch();
   return launch_status();
+}
+}  // namespace
+
+// Shape of the bucketed path's digit pass: LNT_PASS8_VARIANT = 0 (256 threads x 16 keys, window 16;
+// the default), 1 (window 32), 2 (512 x 8), 3 (384 x 12).
+int run_onesweep_pass8(const PairSource& src, bool first, u64* out_k, double* out_v, u32 n, u32 shift, u32 mask,
+                       const u32* bstart, u32* status, u32* tile_counter, cudaStream_t s) {
+  int v = 0;
+  if (const char* e = getenv("LNT_PASS8_VARIANT")) v = atoi(e);
+  switch (v) {
+    case 1:
+      return launch_pass8<256, 16, 32>(src, first, out_k, out_v, n, shift, mask, bstart, status, tile_counter, s);
+    case 2:
+      return launch_pass8<512, 8, 16>(src, first, out_k, out_v, n, shift, mask, bstart, status, tile_counter, s);
+    case 3:
+      return launch_pass8<384, 12, 16>(src, first, out_k, out_v, n, shift, mask, bstart, status, tile_counter, s);
+    default:
+      return launch_pass8<256, 16, 16>(src, first, out_k, out_v, n, shift, mask, bstart, status, tile_counter, s);
+  }
 }
 
 int sort_variant_count() { return kNumVariants; }
