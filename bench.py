@@ -52,6 +52,12 @@ def peaks():
     return HBM_FALLBACK_GBS, "fallback"
 
 
+def tuned_value(key: str):
+    """A value the autotuner compiled into the library (libnt_b200/csrc/lnt_tuned.json)."""
+    f = ROOT / "libnt_b200" / "csrc" / "lnt_tuned.json"
+    return json.loads(f.read_text()).get(key) if f.exists() else None
+
+
 def profile_traffic(name: str, key: str = "traffic_bytes_per_pair"):
     """Per-unit DRAM traffic of a kernel from the committed ncu summary
     (line '<key>: X'), or None."""
@@ -597,7 +603,7 @@ def run_batched(args):
     config = {"workload": "4096 independent lattice products a(i,j,k)*b(k,l,j): dims U{16..512}, nnz log-U[1e2,1e5] "
                           "per operand, f64 U[-1,1]; one CUDA graph of the batched pipeline (persistent SPA kernels)",
               "problems": len(dims), "products": products, "output_nnz": out_total,
-              "queue_chunk": os.environ.get("LNT_BATCH_CHUNK", "8")}
+              "queue_chunk": os.environ.get("LNT_BATCH_CHUNK") or tuned_value("batch_chunk")}
     print(json.dumps(_line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
         "per_contraction_loop": {"problems": loop_n, "ms": loop_s * 1e3,
                                  "products_per_s": lp / loop_s,

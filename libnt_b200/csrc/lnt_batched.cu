@@ -24,6 +24,7 @@
 #include <cstdlib>
 #include <vector>
 
+#include "lnt_tuned.h"
 #include "lnt_scan.cuh"
 
 namespace lnt {
@@ -247,7 +248,7 @@ u32 batch_chunk() {
     const int c = atoi(e);
     if (c >= 1 && c <= 4096) return (u32)c;
   }
-  return 8;
+  return kTunedBatchChunk;
 }
 
 }  // namespace

@@ -487,11 +487,11 @@ int launch_pass8(const PairSource& src, bool first, u64* out_k, double* out_v, u
 }
 }  // namespace
 
-// Shape of the bucketed path's digit pass: LNT_PASS8_VARIANT = 0 (256 threads x 16 keys, window 16;
-// the default), 1 (window 32), 2 (512 x 8), 3 (384 x 12).
+// Shape of the bucketed path's digit pass: 0 (256 threads x 16 keys, window 16), 1 (window 32),
+// 2 (512 x 8), 3 (384 x 12); the tuned choice, or LNT_PASS8_VARIANT from the environment.
 int run_onesweep_pass8(const PairSource& src, bool first, u64* out_k, double* out_v, u32 n, u32 shift, u32 mask,
                        const u32* bstart, u32* status, u32* tile_counter, cudaStream_t s) {
-  int v = 0;
+  int v = kTunedPass8Variant;
   if (const char* e = getenv("LNT_PASS8_VARIANT")) v = atoi(e);
   switch (v) {
     case 1:

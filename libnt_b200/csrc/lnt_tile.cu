@@ -9,7 +9,7 @@
 //   A row-major: A re-keyed to c + w*(r + h*t) and radix-sorted, with row
 //     pointers (h*d + 1);
 //   B row-major: B re-keyed to j + wB*(c + w*t), sorted, duplicate keys
-//     summed, with row pointers (w*d + 1); a row holding at least a quarter of
+//     summed, with row pointers (w*d + 1); a row holding at least an eighth of
 //     its columns is also expanded into a dense row of Bd (one slot per such
 //     row, zero-filled, padded to whole 256-column tiles); for every row
 //     tp[row][q] = position in B of the row's first entry at or right of
@@ -37,6 +37,7 @@
 
 #include "lnt_scan.cuh"
 #include "lnt_sort.cuh"
+#include "lnt_tuned.h"
 
 namespace lnt {
 
@@ -76,8 +77,18 @@ constexpr size_t kStageBytes = (size_t)kPanelRows * kStageStride * 8;
 constexpr size_t kNumericSmem = kStageBytes + (size_t)kTileWarps * 32 * (sizeof(DenseItem) + sizeof(SparseItem));
 constexpr size_t kMaxBitmapBytes = 16ull << 30;
 
+// A B row is expanded into a dense row when div * len >= max(wB, kTileCols):
+// div = LNT_TILE_DENSE_DIV from the environment (1..64), else the tuned value
+// (on the full skewed contraction: 4 -> 70.0 ms, 8 -> 67.7 ms, 16 -> 68.8 ms).
+int dense_div() {
+  const char* e = std::getenv("LNT_TILE_DENSE_DIV");
+  const int v = e ? std::atoi(e) : kTunedTileDenseDiv;
+  return v >= 1 && v <= 64 ? v : kTunedTileDenseDiv;
+}
+
 struct TileDims {
   u64 h, w, wB, d;
+  u64 div;     // dense-row threshold divisor
   u32 nt, nw, np;  // 256-column tiles per row, 64-column bitmap words per row, 32-row panels per tab
   u64 smax;    // dense-row slots
 };
@@ -91,8 +102,9 @@ TileDims tile_dims(u64 h, u64 w, u64 wB, u64 d, u64 nb) {
   t.nt = (u32)((wB + kTileCols - 1) / kTileCols);
   t.nw = (u32)((wB + kWordCols - 1) / kWordCols);
   t.np = (u32)((h + kPanelRows - 1) / kPanelRows);
-  const u64 thr = std::max<u64>(wB, kTileCols);  // dense: 4 * len >= thr
-  t.smax = std::min<u64>(w * d, 4 * nb / thr);
+  t.div = (u64)dense_div();
+  const u64 thr = std::max<u64>(wB, kTileCols);  // dense: div * len >= thr
+  t.smax = std::min<u64>(w * d, t.div * nb / thr);
   return t;
 }
 
@@ -152,13 +164,13 @@ __global__ void tile_rowptr_kernel(const u64* __restrict__ keys, u64 n, const u6
 }
 
 // dslot[row] = dense slot of B row `row`, or -1.
-__global__ void tile_slot_kernel(const u64* __restrict__ brow, u64 nrows, u64 thr, u64 smax, int* __restrict__ dslot,
+__global__ void tile_slot_kernel(const u64* __restrict__ brow, u64 nrows, u64 thr, u64 div, u64 smax, int* __restrict__ dslot,
                                  u32* __restrict__ counter) {
   const u64 stride = (u64)gridDim.x * blockDim.x;
   for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += stride) {
     const u64 len = brow[r + 1] - brow[r];
     int slot = -1;
-    if (len * 4 >= thr) {
+    if (len * div >= thr) {
       const u32 s = atomicAdd(counter, 1u);
       if (s < smax) slot = (int)s;
     }
@@ -550,7 +562,7 @@ int run_tile_mult(const u64* akeys, const double* avals, u64 na, const u64* bkey
     return LNT_DEVICE_ERROR;
   {
     ProfScope prof("tile_bprep", s);
-    tile_slot_kernel<<<grid_cap(brows, 256), 256, 0, s>>>(brow, brows, std::max<u64>(wB, kTileCols), t.smax, dslot,
+    tile_slot_kernel<<<grid_cap(brows, 256), 256, 0, s>>>(brow, brows, std::max<u64>(wB, kTileCols), t.div, t.smax, dslot,
                                                          slot_counter);
     tile_bentry_kernel<<<grid_cap(nb, 256), 256, 0, s>>>(bk, bv, d_nb, brow, make_divider(wB), wB, t.nt, t.nw,
                                                         dslot, bbits, tp, bd);

@@ -1,6 +1,7 @@
 // Autotuned kernel choices.  Written by libnt_b200/tune.py from timings on a
-// B200; entries are tried in order, the first whose ranges contain the
-// request wins.  An empty table falls back to the untuned default.
+// B200 (the values come from lnt_tuned.json); sort entries are tried in
+// order, the first whose ranges contain the request wins.  An empty table
+// falls back to the untuned default.
 #pragma once
 
 namespace lnt {
@@ -55,5 +56,12 @@ static const TunedSortEntry kTunedSort[] = {
     {63, 67108864ull, 0},  // 5.742 ms at n=2^26, 63 bits
     {63, 4611686018427387904ull, 0},  // 11.304 ms at n=2^27, 63 bits
 };
+
+// digit-pass shape of the bucketed sort + collect (see run_onesweep_pass8)
+constexpr int kTunedPass8Variant = 0;
+// work-queue chunk of the batched contraction engine (units per grab)
+constexpr unsigned kTunedBatchChunk = 1;
+// dense-row threshold divisor of the tile engine
+constexpr int kTunedTileDenseDiv = 8;
 
 }  // namespace lnt
