@@ -40,7 +40,8 @@ MAX_KEY = 512 ** 4
 INDEX_ORDER = [3, 2, 1, 0]  # c(i,j,k,l) = a(i,j,k,l) + b(l,k,j,i)
 WORKLOAD = ("sparse merge c(i,j,k,l)=a(i,j,k,l)+b(l,k,j,i): order-4 SparseMIA dims 512^4, "
             "2^26 nnz per operand, uniform coordinates, f64 values U[-1,1], both unsorted (sortMerge: "
-            "re-key A to {3,2,1,0}, concatenate, LSD radix sort of 2^27 (u64,f64) pairs, collect duplicates)")
+            "re-key A to {3,2,1,0}, concatenate, radix-sort the 2^27 (u64,f64) pairs, collect duplicates; here a "
+            "bucket histogram, two 8-bit onesweep passes and a per-bucket shared-memory sort with the fold fused)")
 HBM_FALLBACK_GBS = 6650.0
 
 

@@ -74,10 +74,10 @@ def test_tile_engine_shapes(cuda, torch, rng, force_tile, h, w, wB, d, na, nb, z
 
 
 def test_tile_engine_dense_and_sparse_rows(cuda, torch, rng, force_tile, monkeypatch):
-    monkeypatch.setenv("LNT_TILE_DENSE_DIV", "4")
     """B rows on both sides of a dense-row threshold of a quarter of the
     columns (LNT_TILE_DENSE_DIV=4): full rows, rows at the threshold, just below
     it, single-entry rows, empty rows."""
+    monkeypatch.setenv("LNT_TILE_DENSE_DIV", "4")
     h, w, wB = 700, 40, 257
     rows = []
     for c in range(w):
