@@ -233,6 +233,26 @@ LNT_API int lnt_lattice_mult(const lnt_lattice* A, const lnt_lattice* B, const v
                              uint64_t products, void* workspace, size_t workspace_bytes,
                              uint64_t* c_keys, double* c_vals, uint64_t* d_nc, void* stream);
 
+/* Products with no contracted index: outer and element-wise (inter) modes
+ * only.  Replaces SparseMIABase::noLatticeMult / perform_noLatticeMult
+ * (SparseMIABase.h:1701-1826), reached from MIA_Atom::operator* for pure
+ * outer/inter products (MIA_Expr.h:1012-1057).  A is key-sorted under [its
+ * outer modes, the inter modes] and passed as a lattice rows = outer size,
+ * cols = 1, tabs = inter size; B is sorted under [its outer modes, the inter
+ * modes] and passed as rows = 1, cols = its outer size, tabs = inter size.
+ * C(l_outer, r_outer, inter) = a * b for every pair of entries with equal inter
+ * index, key l_outer + |l_outer| (r_outer + |r_outer| inter), written in the
+ * reference's emission order (ascending keys; B entries major, A entries
+ * minor); equal keys are not folded.  Two phases sharing one workspace:
+ * lnt_nolattice_mult_count writes the product count (the output count) to
+ * *d_products, lnt_nolattice_mult writes C.  LNT_BAD_DIMS when cols(A) != 1,
+ * rows(B) != 1 or the tab counts differ. */
+LNT_API int lnt_nolattice_mult_workspace(const lnt_lattice* A, const lnt_lattice* B, size_t* bytes);
+LNT_API int lnt_nolattice_mult_count(const lnt_lattice* A, const lnt_lattice* B, void* workspace,
+                                     size_t workspace_bytes, uint64_t* d_products, void* stream);
+LNT_API int lnt_nolattice_mult(const lnt_lattice* A, const lnt_lattice* B, uint64_t products, void* workspace,
+                               size_t workspace_bytes, uint64_t* c_keys, double* c_vals, void* stream);
+
 /* ---- batched lattice products ------------------------------------------- */
 
 /* `count` independent products C_p = A_p * B_p, each as lnt_lattice_mult,

@@ -89,6 +89,9 @@ _SIGS = {
                                    C.c_int),
     "lnt_lattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, C.c_uint64, _vp, _sz, _vp, _vp, _vp, _vp],
                          C.c_int),
+    "lnt_nolattice_mult_workspace": ([C.POINTER(Lattice), C.POINTER(Lattice), C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_nolattice_mult_count": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, _sz, _vp, _vp], C.c_int),
+    "lnt_nolattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), C.c_uint64, _vp, _sz, _vp, _vp, _vp], C.c_int),
     "lnt_batched_workspace": ([C.c_int, _vp, _vp, _vp, C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)], C.c_int),
     "lnt_batched_prepare": ([C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
     "lnt_batched_lattice_mult": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp], C.c_int),
@@ -348,6 +351,28 @@ def lattice_mult(a_keys, a_vals, b_keys, b_vals, h: int, w: int, wB: int, d: int
                                   _ptr(cv), _ptr(nc), _stream()), "lnt_lattice_mult")
     m = int(nc.item())
     return ck[:m], cv[:m], products
+
+
+def nolattice_mult(a_keys, a_vals, b_keys, b_vals, h: int, wB: int, d: int = 1):
+    """Product with no contracted index (noLatticeMult): A key-sorted as an
+    h x 1 x d lattice, B as 1 x wB x d; returns (keys, vals) of C (h x wB x d),
+    ascending, equal keys not folded."""
+    torch = _torch()
+    A = Lattice.of(a_keys, a_vals, h, 1, d)
+    B = Lattice.of(b_keys, b_vals, 1, wB, d)
+    dev = a_keys.device
+    b = C.c_size_t(0)
+    _check(lib().lnt_nolattice_mult_workspace(C.byref(A), C.byref(B), C.byref(b)), "lnt_nolattice_mult_workspace")
+    ws = workspace(b.value, dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    _check(lib().lnt_nolattice_mult_count(C.byref(A), C.byref(B), _ptr(ws), ws.numel(), _ptr(cnt), _stream()),
+           "lnt_nolattice_mult_count")
+    n = int(cnt.item())
+    ck = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    cv = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+    _check(lib().lnt_nolattice_mult(C.byref(A), C.byref(B), n, _ptr(ws), ws.numel(), _ptr(ck), _ptr(cv), _stream()),
+           "lnt_nolattice_mult")
+    return ck[:n], cv[:n]
 
 
 class Batch:

@@ -451,3 +451,97 @@ int lnt_lattice_mult(const lnt_lattice* a, const lnt_lattice* b, const void* pla
 }
 
 }  // extern "C"
+
+// ---- noLatticeMult ----------------------------------------------------------
+// Products with no contracted index (SparseMIABase::perform_noLatticeMult,
+// SparseMIABase.h:1716-1826): A as a lattice (h = its outer size) x 1 x d and B
+// as 1 x wB x d (d = the inter size), both key-sorted.  Expanding every B
+// entry's products against the A entries of its tab (expand_kernel with w = 1)
+// yields them in the reference's emission order - B entries major, A entries
+// minor, tab by tab - which is ascending key order, so C needs neither a sort
+// nor a fold (equal keys from operands with duplicate keys stay separate, as
+// in the reference).
+namespace lnt {
+namespace {
+struct NoLatLayout {
+  size_t off_aptr, off_boff, off_scan, total;
+};
+NoLatLayout nolat_layout(const Shape& s) {
+  NoLatLayout L;
+  size_t off = 0;
+  L.off_aptr = off;
+  off += align_up(s.dense_a ? (s.w * s.d + 1) * 8 : 8, 256);
+  L.off_boff = off;
+  off += align_up((s.B.nnz + 1) * 8, 256);
+  L.off_scan = off;
+  off += align_up(scan::workspace_bytes(s.B.nnz), 256);
+  L.total = off;
+  return L;
+}
+int nolat_shape(const lnt_lattice* a, const lnt_lattice* b, Shape* s) {
+  int st = check_shape(a, b, s);
+  if (st != LNT_OK) return st;
+  if (s->w != 1) return LNT_BAD_DIMS;  // A: h x 1 x d, B: 1 x wB x d
+  return LNT_OK;
+}
+}  // namespace
+}  // namespace lnt
+
+extern "C" {
+
+int lnt_nolattice_mult_workspace(const lnt_lattice* a, const lnt_lattice* b, size_t* bytes) {
+  Shape s;
+  int st = nolat_shape(a, b, &s);
+  if (st != LNT_OK) return st;
+  if (!bytes) return LNT_BAD_ARG;
+  *bytes = nolat_layout(s).total;
+  return LNT_OK;
+}
+
+int lnt_nolattice_mult_count(const lnt_lattice* a, const lnt_lattice* b, void* workspace, size_t workspace_bytes,
+                             uint64_t* d_products, void* stream) {
+  Shape s;
+  int st = nolat_shape(a, b, &s);
+  if (st != LNT_OK) return st;
+  if (!d_products) return LNT_BAD_ARG;
+  const NoLatLayout L = nolat_layout(s);
+  if (!workspace || workspace_bytes < L.total || (uintptr_t)workspace % 256) return LNT_WORKSPACE;
+  cudaStream_t cs = as_stream(stream);
+  unsigned char* p = static_cast<unsigned char*>(workspace);
+  u64* aptr = reinterpret_cast<u64*>(p + L.off_aptr);
+  if (s.dense_a) {
+    ProfScope prof("spgemm_colptr", cs);
+    colptr_kernel<<<grid_for(s.A.nnz + 1, 256), 256, 0, cs>>>(s.A.keys, s.A.nnz, make_divider(s.h), s.w * s.d, aptr);
+    count_launch();
+  }
+  AColumns ac{s.dense_a ? aptr : nullptr, s.A.keys, s.A.nnz, s.h};
+  ProductCount pc{ac, s.B.keys, make_divider(s.w), make_divider(s.wB), s.w};
+  st = scan::run(pc, s.B.nnz, (unsigned long long*)(p + L.off_boff), (unsigned long long*)d_products,
+                 p + L.off_scan, cs, "spgemm_count");
+  if (st != LNT_OK) return st;
+  return launch_status();
+}
+
+int lnt_nolattice_mult(const lnt_lattice* a, const lnt_lattice* b, uint64_t products, void* workspace,
+                       size_t workspace_bytes, uint64_t* c_keys, double* c_vals, void* stream) {
+  Shape s;
+  int st = nolat_shape(a, b, &s);
+  if (st != LNT_OK) return st;
+  const NoLatLayout L = nolat_layout(s);
+  if (!workspace || workspace_bytes < L.total || (uintptr_t)workspace % 256) return LNT_WORKSPACE;
+  if (products == 0) return LNT_OK;
+  if (!c_keys || !c_vals) return LNT_BAD_ARG;
+  cudaStream_t cs = as_stream(stream);
+  unsigned char* p = static_cast<unsigned char*>(workspace);
+  AColumns ac{s.dense_a ? reinterpret_cast<const u64*>(p + L.off_aptr) : nullptr, s.A.keys, s.A.nnz, s.h};
+  {
+    ProfScope prof("nolattice_expand", cs);
+    expand_kernel<<<grid_for(products, 256), 256, 0, cs>>>(s.A, s.B, ac, reinterpret_cast<const u64*>(p + L.off_boff),
+                                                          products, make_divider(s.w), make_divider(s.wB),
+                                                          (u64*)c_keys, c_vals);
+    count_launch();
+  }
+  return launch_status();
+}
+
+}  // extern "C"

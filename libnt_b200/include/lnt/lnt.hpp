@@ -509,10 +509,54 @@ inline SparseExpr merge(SparseAtom& a, SparseAtom& b, int op) {
   return {std::move(c), a.labels};
 }
 
+// MIA_Atom::operator* for pure outer / element-wise products (MIA_Expr.h:
+// 1012-1057) -> SparseMIABase::noLatticeMult (SparseMIABase.h:1701-1826): both
+// operands are sorted in place under [outer, inter] (and stay flagged sorted),
+// C = [a outer, b outer, inter] comes out sorted, equal keys are not folded.
+inline SparseExpr nolattice_product(SparseAtom& a, SparseAtom& b, const ProductOrders& o) {
+  SparseTensor bcopy;
+  SparseTensor* bp = b.m;
+  if (a.m == b.m) {  // the product sorts both operands: multiply by a copy (SparseMIABase.h:1706-1710)
+    bcopy = *b.m;
+    bp = &bcopy;
+  }
+  for (size_t q = 0; q < o.l_inter.size(); ++q)
+    if (a.m->dim(o.l_inter[q]) != bp->dim(o.r_inter[q]))
+      throw DimensionMismatchException("Element-wise dimensions must match during MIA multiplication");
+  std::vector<int> sa = o.l_outer, sb = o.r_outer;
+  sa.insert(sa.end(), o.l_inter.begin(), o.l_inter.end());
+  sb.insert(sb.end(), o.r_inter.begin(), o.r_inter.end());
+  a.m->sort(sa);
+  bp->sort(sb);
+  const int64_t d = (int64_t)prod_dims(*a.m, o.l_inter);
+  lnt_lattice A{a.m->keys(), a.m->vals(), a.m->size(), (int64_t)prod_dims(*a.m, o.l_outer), 1, d};
+  lnt_lattice B{bp->keys(), bp->vals(), bp->size(), 1, (int64_t)prod_dims(*bp, o.r_outer), d};
+  size_t need = 0;
+  check(lnt_nolattice_mult_workspace(&A, &B, &need), "product");
+  void* ws = scratch(need);
+  DeviceBuffer<uint64_t> cnt(1);
+  check(lnt_nolattice_mult_count(&A, &B, ws, need, cnt.data(), nullptr), "product");
+  const uint64_t n = read_u64(cnt.data());
+  DeviceBuffer<uint64_t> k(std::max<uint64_t>(n, 1));
+  DeviceBuffer<double> v(std::max<uint64_t>(n, 1));
+  check(lnt_nolattice_mult(&A, &B, n, ws, need, k.data(), v.data(), nullptr), "product");
+  k.shrink(n);
+  v.shrink(n);
+  std::vector<int64_t> dims;
+  Labels labels;
+  for (int i : o.l_outer) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  for (int j : o.r_outer) dims.push_back(bp->dim(j)), labels.push_back(b.labels[j]);
+  for (int i : o.l_inter) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  SparseTensor c(dims);
+  c.take(std::move(k), std::move(v));
+  c.setSorted(true);  // C.setSorted(true) (SparseMIABase.h:1822)
+  return {std::move(c), std::move(labels)};
+}
+
 // MIA_Atom::operator* for the lattice case (MIA_Expr.h:864-925) -> csc_no_accum.
 inline SparseExpr product(SparseAtom& a, SparseAtom& b) {
   const ProductOrders o = product_orders(a.labels, b.labels);
-  if (o.l_inner.empty()) throw MIAParameterException("outer/element-wise-only products are not on this path");
+  if (o.l_inner.empty()) return nolattice_product(a, b, o);
   SparseTensor bcopy;
   SparseTensor* bp = b.m;
   if (a.m == b.m) {  // check_if_copy_needed (MIA_Expr.h:767-802)

@@ -406,25 +406,62 @@ def to_lattice(m: SparseMIA, rows, cols, tabs):
     return m.keys, m.vals, h, w, d
 
 
+def nolattice_mult(ak, av, h, d, bk, bv, wB):
+    """Core of SparseMIABase::perform_noLatticeMult (SparseMIABase.h:1749-1820):
+    A key-sorted as outer + h * inter, B as outer + wB * inter; for each inter
+    index present in both, every (B entry, A entry) pair, B major: key
+    a_outer + b_outer * h + inter * h * wB, value a * b.  No fold of equal keys;
+    the result is ascending."""
+    ak = np.asarray(ak, np.uint64)
+    bk = np.asarray(bk, np.uint64)
+    av = np.asarray(av, np.float64)
+    bv = np.asarray(bv, np.float64)
+    ga, gb = ak // np.uint64(h), bk // np.uint64(wB)
+    common = np.intersect1d(np.unique(ga), np.unique(gb))
+    keys, vals = [], []
+    for g in common:
+        a0, a1 = np.searchsorted(ga, g, "left"), np.searchsorted(ga, g, "right")
+        b0, b1 = np.searchsorted(gb, g, "left"), np.searchsorted(gb, g, "right")
+        ao = (ak[a0:a1] % np.uint64(h)).astype(np.uint64)
+        bo = (bk[b0:b1] % np.uint64(wB)).astype(np.uint64)
+        k = ao[None, :] + np.uint64(h) * bo[:, None] + np.uint64(g) * np.uint64(h) * np.uint64(wB)
+        keys.append(k.ravel())
+        vals.append((av[a0:a1][None, :] * bv[b0:b1][:, None]).ravel())
+    if not keys:
+        return np.zeros(0, np.uint64), np.zeros(0, np.float64)
+    return np.concatenate(keys), np.concatenate(vals)
+
+
 def product(a: SparseMIA, a_labels, b: SparseMIA, b_labels):
-    """Lattice product a(a_labels) * b(b_labels) (MIA_Atom::operator*,
-    MIA_Expr.h:864-925) for the case with inner indices and a sparse result.
+    """Product a(a_labels) * b(b_labels) (MIA_Atom::operator*, MIA_Expr.h:
+    864-925 with inner indices: a lattice product; 1012-1057 without: noLatticeMult).
     Returns (C, c_labels); C has dims [a outer, b outer, inter], the default
     linIdxSequence and sorted = True (SparseMIA.h:362-372)."""
     o = product_orders(a_labels, b_labels)
-    if not o["l_inner"]:
-        raise NotImplementedError("pure outer / element-wise products are not on the lattice path")
     if a is b:
         b = b.copy()  # MIA_Atom::check_if_copy_needed (MIA_Expr.h:767-802)
+    dims = [a.dims[i] for i in o["l_outer"]] + [b.dims[j] for j in o["r_outer"]] + \
+           [a.dims[i] for i in o["l_inter"]]
+    labels = [a_labels[i] for i in o["l_outer"]] + [b_labels[j] for j in o["r_outer"]] + \
+             [a_labels[i] for i in o["l_inter"]]
+    if not o["l_inner"]:
+        # pure outer / element-wise product: noLatticeMult (MIA_Expr.h:1012-1057,
+        # SparseMIABase.h:1701-1826): both operands sorted (in place) under
+        # [outer, inter], no lattice, C sorted by construction
+        if [a.dims[i] for i in o["l_inter"]] != [b.dims[j] for j in o["r_inter"]]:
+            raise ValueError("Element-wise dimensions must match during MIA multiplication")
+        a.sort(list(o["l_outer"]) + list(o["l_inter"]))
+        b.sort(list(o["r_outer"]) + list(o["r_inter"]))
+        h = int(np.prod([a.dims[i] for i in o["l_outer"]], dtype=np.int64)) if o["l_outer"] else 1
+        wB = int(np.prod([b.dims[j] for j in o["r_outer"]], dtype=np.int64)) if o["r_outer"] else 1
+        d = int(np.prod([a.dims[i] for i in o["l_inter"]], dtype=np.int64)) if o["l_inter"] else 1
+        ck, cv = nolattice_mult(a.keys, a.vals, h, d, b.keys, b.vals, wB)
+        return SparseMIA(dims, ck, cv, list(range(len(dims))), True), labels
     ak, av, h, w, d = to_lattice(a, o["l_outer"], o["l_inner"], o["l_inter"])
     bk, bv, hb, wB, db = to_lattice(b, o["r_inner"], o["r_outer"], o["r_inter"])
     if hb != w or db != d:
         raise ValueError("lattice dimension mismatch")
     ck, cv = lattice_mult(ak, av, h, w, d, bk, bv, wB)
-    dims = [a.dims[i] for i in o["l_outer"]] + [b.dims[j] for j in o["r_outer"]] + \
-           [a.dims[i] for i in o["l_inter"]]
-    labels = [a_labels[i] for i in o["l_outer"]] + [b_labels[j] for j in o["r_outer"]] + \
-             [a_labels[i] for i in o["l_inter"]]
     return SparseMIA(dims, ck, cv, list(range(len(dims))), True), labels
 
 

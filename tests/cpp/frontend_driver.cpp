@@ -6,8 +6,8 @@
 //   frontend_driver <scenario> <dir>
 // Files: <name>.keys (uint64), <name>.vals (float64), <name>.meta (text:
 // order, dims..., seq..., sorted).  Scenarios: product, product_assign,
-// elementwise, merge_add, merge_sub, merge_self, plus_equals, sort_seq,
-// collect, dense.
+// elementwise, outer_inter, outer, merge_add, merge_sub, merge_self,
+// plus_equals, sort_seq, collect, dense.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -94,6 +94,24 @@ int main(int argc, char** argv) {
       load(b, "b");
       d(i, l, !n) = a(i, j, !n) * b(j, l, !n);
       save(d, "c");
+    } else if (sc == "outer_inter") {  // noLatticeMult: outer i, l with element-wise n
+      lnt::SparseNT<2> a, b;
+      lnt::SparseNT<3> d;
+      load(a, "a");
+      load(b, "b");
+      d(i, l, !n) = a(i, !n) * b(!n, l);
+      save(d, "c");
+      save(a, "a_after");
+      save(b, "b_after");
+    } else if (sc == "outer") {  // noLatticeMult: pure outer product
+      lnt::SparseNT<2> a, b;
+      lnt::SparseNT<4> d;
+      load(a, "a");
+      load(b, "b");
+      d(i, j, k, l) = a(i, j) * b(k, l);
+      save(d, "c");
+      save(a, "a_after");
+      save(b, "b_after");
     } else if (sc == "merge_add" || sc == "merge_sub") {
       lnt::SparseNT<4> a, b, c;
       load(a, "a");

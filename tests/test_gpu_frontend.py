@@ -87,6 +87,25 @@ def test_elementwise_product(driver, tmp_path, rng):
     same(read(tmp_path, "c"), c)
 
 
+@pytest.mark.parametrize("scenario,a_lab,b_lab,a_dims,b_dims", [
+    ("outer_inter", ["i", "!n"], ["!n", "l"], [40, 9], [9, 30]),
+    ("outer", ["i", "j"], ["k", "l"], [15, 12], [12, 14]),
+])
+def test_nolattice_product(driver, tmp_path, rng, scenario, a_lab, b_lab, a_dims, b_dims):
+    """d(i,l,!n) = a(i,!n) * b(!n,l) and d(i,j,k,l) = a(i,j) * b(k,l): noLatticeMult,
+    with both operands sorted in place under [outer, inter] as side effect."""
+    a = rand_mia(rng, a_dims, 150)
+    b = rand_mia(rng, b_dims, 120)
+    write(tmp_path, "a", a)
+    write(tmp_path, "b", b)
+    run(driver, scenario, tmp_path)
+    ea, eb = a.copy(), b.copy()
+    c, _ = oracle.product(ea, a_lab, eb, b_lab)
+    same(read(tmp_path, "c"), c, atol=0)
+    same(read(tmp_path, "a_after"), ea, atol=0)
+    same(read(tmp_path, "b_after"), eb, atol=0)
+
+
 @pytest.mark.parametrize("a_state,b_state", [("unsorted", "unsorted"), ("sorted", "unsorted"),
                                              ("unsorted", "sorted"), ("sorted", "sorted"),
                                              ("sorted_other", "unsorted"), ("unsorted", "sorted_other")])

@@ -237,3 +237,51 @@ def test_lattice_mult_cross_check_dense(rng):
         Cd = np.zeros(h * wB * d)
         Cd[ck.astype(np.int64)] = cv
         np.testing.assert_allclose(Cd, np.einsum("rkt,kct->rct", A, B).ravel(order="F"), atol=1e-12)
+
+
+# ---- noLatticeMult (pure outer / element-wise products) ---------------------
+
+def _sparse_operand(rng, dims, density=0.4):
+    dense = np.where(rng.random(dims) < density, rng.uniform(-1, 1, dims), 0.0)
+    idx = np.nonzero(dense.reshape(dims, order="F").ravel(order="F"))[0]  # LCO key, first mode fastest
+    return dense, idx.astype(np.uint64), dense.ravel(order="F")[idx]
+
+
+@pytest.mark.parametrize("a_lab,b_lab", [
+    (["i", "!k"], ["j", "!k"]),            # outer i, j with element-wise k
+    (["i", "j"], ["k", "l"]),              # pure outer
+    (["!i", "!j"], ["!i", "!j"]),          # element-wise only
+    (["i", "!k", "!m"], ["!m", "j", "!k"]),  # two inter modes, permuted in b
+])
+def test_nolattice_product_vs_dense(a_lab, b_lab):
+    """c = a * b without contracted indices (noLatticeMult, SparseMIABase.h:1716-1826):
+    C dims [a outer, b outer, inter], sorted, values = products of the dense operands."""
+    rng = np.random.default_rng(5)
+    size = {"i": 5, "j": 4, "k": 6, "l": 3, "m": 2}
+    a_dims = [size[l.lstrip("!")] for l in a_lab]
+    b_dims = [size[l.lstrip("!")] for l in b_lab]
+    Ad, ak, av = _sparse_operand(rng, a_dims)
+    Bd, bk, bv = _sparse_operand(rng, b_dims)
+    a = oracle.SparseMIA(a_dims, ak, av, sorted=False)
+    b = oracle.SparseMIA(b_dims, bk, bv, sorted=False)
+    c, c_lab = oracle.product(a, list(a_lab), b, list(b_lab))
+    assert c.sorted and np.all(np.diff(c.keys.astype(np.int64)) > 0)
+    letters = {l.lstrip("!"): chr(ord("a") + n) for n, l in enumerate(sorted(size))}
+    sub = lambda labs: "".join(letters[l.lstrip("!")] for l in labs)
+    Cd = np.einsum(f"{sub(a_lab)},{sub(b_lab)}->{sub(c_lab)}", Ad, Bd)
+    got = np.zeros(int(np.prod(c.dims)))
+    got[c.keys.astype(np.int64)] = c.vals
+    np.testing.assert_array_equal(got.reshape(c.dims, order="F"), Cd)
+    # every pair of non-zeros with equal inter indices is an entry (values are non-zero)
+    assert c.keys.size == np.count_nonzero(Cd)
+    o = oracle.product_orders(list(a_lab), list(b_lab))
+    assert a.seq == o["l_outer"] + o["l_inter"] and b.seq == o["r_outer"] + o["r_inter"]
+
+
+def test_nolattice_keeps_duplicate_products():
+    """Operands that are not sets: every product is its own entry (no fold)."""
+    a = oracle.SparseMIA([3, 2], np.array([0, 0, 4], np.uint64), np.array([1.0, 2.0, 3.0]), sorted=False)
+    b = oracle.SparseMIA([2, 2], np.array([1, 1], np.uint64), np.array([5.0, 7.0]), sorted=False)
+    c, _ = oracle.product(a, ["i", "!k"], b, ["j", "!k"])   # k = 0 for all entries except a key 4 (k = 1)
+    np.testing.assert_array_equal(c.keys, np.array([3, 3, 3, 3], np.uint64))
+    np.testing.assert_array_equal(c.vals, np.array([5.0, 10.0, 7.0, 14.0]))
