@@ -253,6 +253,27 @@ LNT_API int lnt_nolattice_mult_count(const lnt_lattice* A, const lnt_lattice* B,
 LNT_API int lnt_nolattice_mult(const lnt_lattice* A, const lnt_lattice* B, uint64_t products, void* workspace,
                                size_t workspace_bytes, uint64_t* c_keys, double* c_vals, void* stream);
 
+/* Unary contraction / attraction: SparseMIABase::contract_attract
+ * (SparseMIABase.h:1913-2053), which MIA_Atom applies to index labels repeated
+ * inside one operand (perform_unary, MIA_Expr.h:690-735).  keys/vals: the
+ * tensor sorted under the sequence [contraction modes, attraction modes, other
+ * modes]; sdims[0..order): the extents in that sequence.  The first modes form
+ * ncon_sets contraction sets of con_part[p] modes each (summed along their
+ * diagonal), the next natt_sets attraction sets of att_part[p] modes (their
+ * diagonal becomes one output mode); the rest are kept.  Output, in the
+ * reference's emission order: one entry per group of equal kept and attracted
+ * indices whose attraction sets agree and whose sum over the entries with
+ * agreeing contraction sets is not zero; key = kept linear index + |kept| *
+ * attraction linear index (output extents [kept..., one per attraction set]).
+ * *d_nout = output count (<= n); *d_sorted (optional) = non-zero when the keys
+ * written never decrease (the result's sorted flag).  LNT_BAD_DIMS when a set
+ * spans different extents. */
+LNT_API int lnt_contract_attract_workspace(size_t n, size_t* bytes);
+LNT_API int lnt_contract_attract(const uint64_t* keys, const double* vals, size_t n, int order,
+                                 const int64_t* sdims, int ncon_sets, const int* con_part, int natt_sets,
+                                 const int* att_part, uint64_t* out_keys, double* out_vals, uint64_t* d_nout,
+                                 uint32_t* d_sorted, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- batched lattice products ------------------------------------------- */
 
 /* `count` independent products C_p = A_p * B_p, each as lnt_lattice_mult,

@@ -89,6 +89,9 @@ _SIGS = {
                                    C.c_int),
     "lnt_lattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, C.c_uint64, _vp, _sz, _vp, _vp, _vp, _vp],
                          C.c_int),
+    "lnt_contract_attract_workspace": ([_sz, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_contract_attract": ([_vp, _vp, _sz, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
+                              _vp], C.c_int),
     "lnt_nolattice_mult_workspace": ([C.POINTER(Lattice), C.POINTER(Lattice), C.POINTER(C.c_size_t)], C.c_int),
     "lnt_nolattice_mult_count": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, _sz, _vp, _vp], C.c_int),
     "lnt_nolattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), C.c_uint64, _vp, _sz, _vp, _vp, _vp], C.c_int),
@@ -373,6 +376,31 @@ def nolattice_mult(a_keys, a_vals, b_keys, b_vals, h: int, wB: int, d: int = 1):
     _check(lib().lnt_nolattice_mult(C.byref(A), C.byref(B), n, _ptr(ws), ws.numel(), _ptr(ck), _ptr(cv), _stream()),
            "lnt_nolattice_mult")
     return ck[:n], cv[:n]
+
+
+def contract_attract(keys, vals, sdims, con_part, att_part):
+    """Unary contraction / attraction of a tensor sorted under [contraction
+    modes, attraction modes, other modes] (extents sdims in that order);
+    returns (keys, vals, sorted_flag)."""
+    torch = _torch()
+    _dev(keys), _dev(vals)
+    n = keys.numel()
+    dev = keys.device
+    b = C.c_size_t(0)
+    _check(lib().lnt_contract_attract_workspace(n, C.byref(b)), "lnt_contract_attract_workspace")
+    ws = workspace(b.value, dev)
+    ok = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    ov = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    flag = torch.zeros(1, dtype=torch.int32, device=dev)
+    sd = np.ascontiguousarray(sdims, np.int64)
+    cp = np.ascontiguousarray(con_part, np.int32)
+    ap = np.ascontiguousarray(att_part, np.int32)
+    _check(lib().lnt_contract_attract(_ptr(keys), _ptr(vals), n, len(sd), sd.ctypes.data, len(cp), cp.ctypes.data,
+                                      len(ap), ap.ctypes.data, _ptr(ok), _ptr(ov), _ptr(cnt), _ptr(flag), _ptr(ws),
+                                      ws.numel(), _stream()), "lnt_contract_attract")
+    m = int(cnt.item())
+    return ok[:m], ov[:m], bool(flag.item())
 
 
 class Batch:

@@ -394,6 +394,7 @@ struct SparseExpr {
 struct SparseAtom {
   SparseTensor* m;
   Labels labels;
+  std::shared_ptr<SparseTensor> owned;  // set when the atom holds a contraction / attraction result
 
   // c(...) = expression: relabel only (SparseMIA::assign, SparseMIA.h:891-928)
   SparseAtom& operator=(SparseExpr&& e) {
@@ -623,6 +624,83 @@ inline SparseAtom& SparseAtom::operator-=(const SparseAtom& o) {
   return *this;
 }
 
+namespace detail {
+
+// Repeated labels inside one operand (perform_unary, MIA_Expr.h:690-735):
+// classification as unary_helper (MIA_Expr.h:632-662) with
+// pull_contract_indices / pull_attract_indices / pull_sequence_from_list
+// (ExprUtil.h:80-300) - a plain label repeated is contracted, an element-wise
+// label repeated among the rest is attracted, sets in the order of their
+// labels' last occurrences, positions ascending - then
+// SparseMIABase::contract_attract (SparseMIABase.h:1913-2053): the operand is
+// sorted in place under [contract, attract, other]; the result has modes
+// [other..., one per attraction] and its sorted flag as push_back leaves it.
+inline SparseAtom unary(SparseTensor& t, Labels labels) {
+  auto count = [](const Labels& seq, const Index& x) {
+    return (int)std::count(seq.begin(), seq.end(), x);
+  };
+  auto pull = [&](const Labels& seq, bool elem, Labels& found, Labels& rest) {
+    for (size_t q = seq.size(); q-- > 0;)
+      if (count(seq, seq[q]) > 1 && seq[q].elementwise() == elem && !count(found, seq[q]))
+        found.insert(found.begin(), seq[q]);
+    for (const Index& x : seq)
+      if (!(count(seq, x) > 1 && x.elementwise() == elem)) rest.push_back(x);
+  };
+  Labels con, rest1, att, rest2;
+  pull(labels, false, con, rest1);
+  pull(rest1, true, att, rest2);
+  if (con.empty() && att.empty()) return SparseAtom{&t, std::move(labels), nullptr};
+  std::vector<int> seq, cpart, apart;
+  auto positions = [&](const Labels& sub, std::vector<int>& part) {
+    for (const Index& x : sub) {
+      int c = 0;
+      for (size_t q = 0; q < labels.size(); ++q)
+        if (labels[q] == x) seq.push_back((int)q), ++c;
+      part.push_back(c);
+    }
+  };
+  positions(con, cpart);
+  positions(att, apart);
+  std::vector<int> other;
+  for (int q = 0; q < (int)labels.size(); ++q)
+    if (std::find(seq.begin(), seq.end(), q) == seq.end()) other.push_back(q);
+  seq.insert(seq.end(), other.begin(), other.end());
+  t.sort(seq);
+  std::vector<int64_t> sdims, rdims;
+  for (int q : seq) sdims.push_back(t.dim(q));
+  for (int q : other) rdims.push_back(t.dim(q));
+  size_t at = 0;
+  for (int q = 0; q < (int)cpart.size(); ++q) at += (size_t)cpart[q];
+  for (int c : apart) {
+    rdims.push_back(sdims[at]);
+    at += (size_t)c;
+  }
+  size_t need = 0;
+  check(lnt_contract_attract_workspace(t.size(), &need), "contract_attract");
+  const size_t n = t.size();
+  DeviceBuffer<uint64_t> k(std::max<size_t>(n, 1));
+  DeviceBuffer<double> v(std::max<size_t>(n, 1));
+  DeviceBuffer<uint64_t> cnt(1);
+  DeviceBuffer<uint32_t> flag(1);
+  check(lnt_contract_attract(t.keys(), t.vals(), n, (int)sdims.size(), sdims.data(), (int)cpart.size(), cpart.data(),
+                             (int)apart.size(), apart.data(), k.data(), v.data(), cnt.data(), flag.data(),
+                             scratch(need), need, nullptr),
+        "contract_attract");
+  const uint64_t m = read_u64(cnt.data());
+  uint32_t sorted = 0;
+  cuda_check(cudaMemcpy(&sorted, flag.data(), 4, cudaMemcpyDeviceToHost), "contract_attract flag");
+  k.shrink(m);
+  v.shrink(m);
+  auto r = std::make_shared<SparseTensor>(rdims);
+  r->take(std::move(k), std::move(v));
+  r->setSorted(sorted != 0);
+  Labels rl = rest2;
+  rl.insert(rl.end(), att.begin(), att.end());
+  return SparseAtom{r.get(), std::move(rl), r};
+}
+
+}  // namespace detail
+
 // SparseNT<N> / SparseMIA<double, N>: a SparseTensor of fixed order N.
 template <size_t N>
 class SparseNT : public SparseTensor {
@@ -632,7 +710,7 @@ class SparseNT : public SparseTensor {
   explicit SparseNT(D... dims) : SparseTensor(std::vector<int64_t>{(int64_t)dims...}) {}
   template <class... I, typename = std::enable_if_t<sizeof...(I) == N>>
   SparseAtom operator()(const I&... idx) {
-    return SparseAtom{this, Labels{idx...}};
+    return detail::unary(*this, Labels{idx...});
   }
   SparseNT& operator=(SparseTensor&& t) {
     if (t.order() != N) throw MIAParameterException("order mismatch");

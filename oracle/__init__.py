@@ -465,6 +465,127 @@ def product(a: SparseMIA, a_labels, b: SparseMIA, b_labels):
     return SparseMIA(dims, ck, cv, list(range(len(dims))), True), labels
 
 
+def unary_orders(labels) -> dict:
+    """Contraction / attraction classification of one operand's labels, a
+    restatement of unary_helper (MIA_Expr.h:632-662) with pull_contract_indices,
+    pull_attract_indices (ExprUtil.h:80-248) and pull_sequence_from_list
+    (ExprUtil.h:250-300): a plain label repeated in the operand is contracted,
+    an element-wise ('!') label repeated among the rest is attracted; sets are
+    listed in the order of their labels' last occurrences, each with its
+    positions ascending.  Result labels: the others, then one per attraction."""
+    labels = list(labels)
+
+    def pull(seq, elem):
+        found = []
+        for q in range(len(seq) - 1, -1, -1):
+            lab = seq[q]
+            if seq.count(lab) > 1 and _is_elem(lab) == elem and lab not in found:
+                found.insert(0, lab)
+        rest = [lab for lab in seq if not (seq.count(lab) > 1 and _is_elem(lab) == elem)]
+        return found, rest
+
+    con, rest1 = pull(labels, False)
+    att, rest2 = pull(rest1, True)
+
+    def positions(sub):
+        pos, part = [], []
+        for lab in sub:
+            ps = [q for q, x in enumerate(labels) if x == lab]
+            pos += ps
+            part.append(len(ps))
+        return pos, part
+
+    cpos, cpart = positions(con)
+    apos, apart = positions(att)
+    other = sorted(set(range(len(labels))) - set(cpos) - set(apos))
+    return dict(contract=cpos, contract_part=cpart, attract=apos, attract_part=apart, other=other,
+                labels=rest2 + att)
+
+
+def contract_attract(m: SparseMIA, cpos, cpart, apos, apart) -> SparseMIA:
+    """SparseMIABase::contract_attract (SparseMIABase.h:1913-2053), loop kept as
+    in the reference: sort m (in place) under [contract, attract, other]; walk
+    the entries; an entry whose attraction sets disagree is skipped; otherwise
+    the run of entries with equal key / contract_dimensionality (equal attract
+    and other indices) is summed over the entries whose contraction sets agree,
+    and a non-zero sum is pushed at key/(contract_dim * attract_dim) +
+    attract_idx * other_dim.  Result dims [other, attraction ranges]; sorted
+    flag as push_back leaves it (SparseMIA.h:570-578)."""
+    order = m.order
+    other = sorted(set(range(order)) - set(cpos) - set(apos))
+    sort_order = list(cpos) + list(apos) + other
+    m.sort(sort_order)
+    sdims = [m.dims[q] for q in sort_order]
+    contract_dim, cur = 1, 0
+    for part in cpart:
+        contract_dim *= m.dims[cpos[cur]] ** part
+        cur += part
+    ranges, attract_dim, cur = [], 1, 0
+    for part in apart:
+        ranges.append(m.dims[apos[cur]])
+        attract_dim *= ranges[-1] ** part
+        cur += part
+    other_dim = int(np.prod([m.dims[q] for q in other], dtype=np.int64)) if other else 1
+
+    def ind2sub(k):
+        out = []
+        for dd in sdims:
+            out.append(k % dd)
+            k //= dd
+        return out
+
+    keys = [int(x) for x in m.keys]
+    vals = m.vals
+    out_k, out_v = [], []
+    ncon = len(cpos)
+    e = 0
+    while e < len(keys):
+        idx = ind2sub(keys[e])
+        ok, start, cur_att = True, ncon, []
+        for part in apart:
+            if any(idx[q] != idx[start] for q in range(start + 1, start + part)):
+                ok = False
+                break
+            cur_att.append(idx[start])
+            start += part
+        if not ok:
+            e += 1
+            continue
+        att_idx, stride = 0, 1
+        for v_, r_ in zip(cur_att, ranges):
+            att_idx += v_ * stride
+            stride *= r_
+        head = keys[e]
+        total = 0.0
+        while e < len(keys) and head // contract_dim == keys[e] // contract_dim:
+            idx = ind2sub(keys[e])
+            add, start = True, 0
+            for part in cpart:
+                if any(idx[q] != idx[start] for q in range(start + 1, start + part)):
+                    add = False
+                    break
+                start += part
+            if add:
+                total += float(vals[e])
+            e += 1
+        if total:
+            out_k.append(head // (contract_dim * attract_dim) + att_idx * other_dim)
+            out_v.append(total)
+    ok_ = np.array(out_k, np.uint64)
+    sorted_ = bool(np.all(ok_[1:] >= ok_[:-1])) if ok_.size > 1 else True
+    dims = [m.dims[q] for q in other] + ranges
+    return SparseMIA(dims, ok_, np.array(out_v, np.float64), list(range(len(dims))), sorted_)
+
+
+def unary(m: SparseMIA, labels):
+    """m(labels) with repeated labels (perform_unary, MIA_Expr.h:690-735):
+    returns (result, result labels); m itself when no label repeats."""
+    o = unary_orders(labels)
+    if not o["contract"] and not o["attract"]:
+        return m, list(labels)
+    return contract_attract(m, o["contract"], o["contract_part"], o["attract"], o["attract_part"]), o["labels"]
+
+
 def assign(dest_labels, src: SparseMIA, src_labels) -> SparseMIA:
     """c(dest_labels) = <expression result with src_labels>: when the label
     orders differ only linIdxSequence and dims are rewritten, no sort

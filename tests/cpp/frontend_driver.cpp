@@ -6,8 +6,8 @@
 //   frontend_driver <scenario> <dir>
 // Files: <name>.keys (uint64), <name>.vals (float64), <name>.meta (text:
 // order, dims..., seq..., sorted).  Scenarios: product, product_assign,
-// elementwise, outer_inter, outer, merge_add, merge_sub, merge_self,
-// plus_equals, sort_seq, collect, dense.
+// elementwise, outer_inter, outer, trace, attract, merge_add, merge_sub,
+// merge_self, plus_equals, sort_seq, collect, dense.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -112,6 +112,20 @@ int main(int argc, char** argv) {
       save(d, "c");
       save(a, "a_after");
       save(b, "b_after");
+    } else if (sc == "trace") {  // contract_attract: double trace
+      lnt::SparseNT<5> a;
+      lnt::SparseNT<1> c;
+      load(a, "a");
+      c(k) = a(i, j, i, j, k);
+      save(c, "c");
+      save(a, "a_after");
+    } else if (sc == "attract") {  // contract_attract: attraction of i, contraction of j
+      lnt::SparseNT<5> a;
+      lnt::SparseNT<2> c;
+      load(a, "a");
+      c(k, !i) = a(!i, j, !i, k, j);
+      save(c, "c");
+      save(a, "a_after");
     } else if (sc == "merge_add" || sc == "merge_sub") {
       lnt::SparseNT<4> a, b, c;
       load(a, "a");

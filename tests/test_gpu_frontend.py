@@ -106,6 +106,24 @@ def test_nolattice_product(driver, tmp_path, rng, scenario, a_lab, b_lab, a_dims
     same(read(tmp_path, "b_after"), eb, atol=0)
 
 
+@pytest.mark.parametrize("scenario,labels,dims,c_labels", [
+    ("trace", ["i", "j", "i", "j", "k"], [6, 5, 6, 5, 7], ["k"]),
+    ("attract", ["!i", "j", "!i", "k", "j"], [6, 5, 6, 7, 5], ["k", "!i"]),
+])
+def test_unary_contract_attract(driver, tmp_path, rng, scenario, labels, dims, c_labels):
+    """c(k) = a(i,j,i,j,k) and c(k,!i) = a(!i,j,!i,k,j): contract_attract, the
+    operand sorted in place under [contract, attract, other], the result's
+    sorted flag as push_back leaves it."""
+    a = rand_mia(rng, dims, 4000)
+    write(tmp_path, "a", a)
+    run(driver, scenario, tmp_path)
+    ea = a.copy()
+    c, lab = oracle.unary(ea, labels)
+    assert lab == c_labels
+    same(read(tmp_path, "c"), c)
+    same(read(tmp_path, "a_after"), ea, atol=0)
+
+
 @pytest.mark.parametrize("a_state,b_state", [("unsorted", "unsorted"), ("sorted", "unsorted"),
                                              ("unsorted", "sorted"), ("sorted", "sorted"),
                                              ("sorted_other", "unsorted"), ("unsorted", "sorted_other")])

@@ -285,3 +285,35 @@ def test_nolattice_keeps_duplicate_products():
     c, _ = oracle.product(a, ["i", "!k"], b, ["j", "!k"])   # k = 0 for all entries except a key 4 (k = 1)
     np.testing.assert_array_equal(c.keys, np.array([3, 3, 3, 3], np.uint64))
     np.testing.assert_array_equal(c.vals, np.array([5.0, 10.0, 7.0, 14.0]))
+
+
+# ---- unary contraction / attraction (contract_attract) -----------------------
+
+@pytest.mark.parametrize("labels,sub", [
+    (["i", "j", "i", "j", "k"], "ijijk->k"),        # double trace
+    (["!i", "j", "!i", "k", "j"], "ijikj->ki"),     # attraction of i, contraction of j
+    (["!i", "k", "!i"], "iki->ki"),                  # attraction only (diagonal kept)
+])
+def test_contract_attract_vs_dense(labels, sub):
+    rng = np.random.default_rng(11)
+    size = {"i": 4, "j": 3, "k": 5}
+    dims = [size[l.lstrip("!")] for l in labels]
+    Ad, ak, av = _sparse_operand(rng, dims, density=0.6)
+    m = oracle.SparseMIA(dims, ak, av, sorted=False)
+    c, lab = oracle.unary(m, labels)
+    o = oracle.unary_orders(labels)
+    assert lab == o["labels"]
+    Cd = np.einsum(sub, Ad)
+    got = np.zeros(int(np.prod(c.dims)))
+    got[c.keys.astype(np.int64)] = c.vals
+    np.testing.assert_allclose(got.reshape(c.dims, order="F"), Cd, rtol=0, atol=1e-12)
+    assert c.keys.size == np.count_nonzero(Cd)
+    assert m.seq == o["contract"] + o["attract"] + o["other"]          # the operand is sorted in place
+    assert c.sorted == bool(np.all(np.diff(c.keys.astype(np.int64)) >= 0))
+
+
+def test_contract_attract_drops_zero_sums():
+    """A group whose diagonal entries cancel exactly is not pushed (if (sum))."""
+    m = oracle.SparseMIA([2, 2, 3], np.array([0, 3, 10], np.uint64), np.array([1.0, -1.0, 5.0]), sorted=False)
+    c, lab = oracle.unary(m, ["i", "i", "k"])   # k = 0: (0,0,0) and (1,1,0) cancel; (0,1,2) is off the diagonal
+    assert lab == ["k"] and c.keys.size == 0
