@@ -733,6 +733,175 @@ def run_dense(args):
     })), flush=True)
     return 0
 
+def _timed_steps(torch, step, args):
+    """W untimed steps, then K timed steps with CUDA events on the current
+    stream (library profiler on); returns ms per step and the launch count."""
+    import libnt_b200 as L
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = L.launch_count()
+    L.profile_reset()
+    L.profile_enable(True)
+    sampler = ClockSampler(torch.cuda.current_device())
+    e0, e1 = _events()
+    with sampler:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    L.profile_enable(False)
+    return e0.elapsed_time(e1) / args.steps, L.launch_count() - launches0, sampler.summary()
+
+
+def run_outer(args):
+    """Product without contracted indices (noLatticeMult): d(i,l,!n) = a(i,!n) * b(!n,l),
+    a 4096 x 65536 with 2^24 entries, b 65536 x 64 with 2^21 entries (uniform,
+    distinct, key-sorted under [outer, inter]); a step = count + expansion
+    through the C ABI.  Output-write bound: 16 B per product."""
+    import ctypes as C
+
+    import torch
+
+    import libnt_b200 as L
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    h, wB, d = 4096, 64, 65536
+    ak = torch.unique(torch.randint(0, h * d, (1 << 24,), generator=g, device=dev))
+    bk = torch.unique(torch.randint(0, wB * d, (1 << 21,), generator=g, device=dev))
+    av = torch.rand(ak.numel(), generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    bv = torch.rand(bk.numel(), generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    A = L.Lattice.of(ak, av, h, 1, d)
+    B = L.Lattice.of(bk, bv, 1, wB, d)
+    lib = L.lib()
+    nb_ = C.c_size_t(0)
+    L._check(lib.lnt_nolattice_mult_workspace(C.byref(A), C.byref(B), C.byref(nb_)), "workspace")
+    ws = L.workspace(nb_.value, dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    L._check(lib.lnt_nolattice_mult_count(C.byref(A), C.byref(B), C.c_void_p(ws.data_ptr()), ws.numel(),
+                                          C.c_void_p(cnt.data_ptr()), stream), "count")
+    P = int(cnt.item())
+    ck = torch.empty(P, dtype=torch.int64, device=dev)
+    cv = torch.empty(P, dtype=torch.float64, device=dev)
+
+    def step():
+        L._check(lib.lnt_nolattice_mult_count(C.byref(A), C.byref(B), C.c_void_p(ws.data_ptr()), ws.numel(),
+                                              C.c_void_p(cnt.data_ptr()), stream), "count")
+        L._check(lib.lnt_nolattice_mult(C.byref(A), C.byref(B), C.c_uint64(P), C.c_void_p(ws.data_ptr()),
+                                        ws.numel(), C.c_void_p(ck.data_ptr()), C.c_void_p(cv.data_ptr()), stream),
+                 "mult")
+
+    ms, launches, clocks = _timed_steps(torch, step, args)
+    exp_ms = L.profile_query("nolattice_expand")[0] / args.steps
+    ms = max_over_ranks(ms, world)
+    # spot check: the first and last products against the inputs
+    k0 = int(ck[0].item())
+    assert L.device_status() == 0 and int(cnt.item()) == P and bool(torch.all(ck[1:] >= ck[:-1]).item())
+    if rank != 0:
+        return 0
+    peak, peak_kind = peaks()
+    alg = 16.0 * (ak.numel() + bk.numel() + P)
+    cpu = None
+    if not args.no_cpu and world == 1:
+        import oracle
+        rng = np.random.default_rng(1)
+        hs, ds = 512, 4096
+        cak = np.unique(rng.integers(0, hs * ds, 1 << 20, dtype=np.uint64))
+        cbk = np.unique(rng.integers(0, wB * ds, 1 << 17, dtype=np.uint64))
+        t0 = time.perf_counter()
+        kk, _ = oracle.nolattice_mult(cak, rng.uniform(-1, 1, cak.size), hs, ds, cbk, rng.uniform(-1, 1, cbk.size), wB)
+        t = time.perf_counter() - t0
+        cpu = {"value": kk.size / t, "unit": "products/s", "cores": 1, "kind": "port",
+               "sample": f"a 512 x 4096 with 2^20 draws, b 64 x 4096 with 2^17 ({kk.size} products): the restated "
+                         "noLatticeMult loop (numpy per inter index), one thread"}
+    config = {"workload": "noLatticeMult d(i,l,!n) = a(i,!n) * b(!n,l): a 4096 x 65536 (2^24 draws), b 65536 x 64 "
+                          "(2^21 draws), uniform, key-sorted; step = count + expansion",
+              "nnz_a": int(ak.numel()), "nnz_b": int(bk.numel()), "products": P, "first_key": k0,
+              "l2": "output far larger than L2", "parallelism": "1 GPU"}
+    print(json.dumps(_line("products/s", P * world / (ms * 1e-3), ms, args, world, config, {
+        "gpu_launches": launches, "cpu_baseline": cpu, "clocks": clocks,
+        "roofline": {"bound": "hbm", "kernel": "nolattice_expand", "achieved": alg / (exp_ms * 1e-3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": alg / (exp_ms * 1e-3) / 1e9 / peak,
+                     "alg_bytes_per_launch": alg, "avg_launch_ms": exp_ms, "peak_source": peak_kind,
+                     "traffic": None},
+    })), flush=True)
+    return 0
+
+
+def run_unary(args):
+    """Unary contraction (contract_attract): b(k) = a(i,i,k), a 8192 x 8192 x 1024
+    with 2^26 entries (uniform, distinct, key-sorted under [i, i, k]); a step =
+    lnt_contract_attract through the C ABI.  HBM bound: 16 B per input entry
+    plus 16 B per output entry."""
+    import torch
+
+    import libnt_b200 as L
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    dims = [8192, 8192, 1024]
+    total = dims[0] * dims[1] * dims[2]
+    keys = torch.unique(torch.randint(0, total, (1 << 26,), generator=g, device=dev))
+    # a tenth of the entries on the diagonal i = i', so the output is not trivial
+    idx = torch.arange(0, keys.numel(), 10, device=dev)
+    i0 = keys[idx] % dims[0]
+    rest = keys[idx] // (dims[0] * dims[1])
+    keys[idx] = i0 + dims[0] * i0 + dims[0] * dims[1] * rest
+    keys = torch.unique(keys)
+    vals = torch.rand(keys.numel(), generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    n = keys.numel()
+    import ctypes as C
+    lib = L.lib()
+    nb_ = C.c_size_t(0)
+    L._check(lib.lnt_contract_attract_workspace(n, C.byref(nb_)), "workspace")
+    ws = L.workspace(nb_.value, dev)
+    ok = torch.empty(n, dtype=torch.int64, device=dev)
+    ov = torch.empty(n, dtype=torch.float64, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    sd = np.array(dims, np.int64)
+    cp = np.array([2], np.int32)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def step():
+        L._check(lib.lnt_contract_attract(C.c_void_p(keys.data_ptr()), C.c_void_p(vals.data_ptr()), n, 3,
+                                          sd.ctypes.data, 1, cp.ctypes.data, 0, None, C.c_void_p(ok.data_ptr()),
+                                          C.c_void_p(ov.data_ptr()), C.c_void_p(cnt.data_ptr()), None,
+                                          C.c_void_p(ws.data_ptr()), ws.numel(), stream), "lnt_contract_attract")
+
+    ms, launches, clocks = _timed_steps(torch, step, args)
+    kernels = {k: L.profile_query(k)[0] / args.steps for k in ("unary_map", "collect_lead", "collect", "unary_scan",
+                                                                 "unary_write")}
+    ms = max_over_ranks(ms, world)
+    m = int(cnt.item())
+    # spot check: output k holds the sum of the diagonal entries a(i,i,k)
+    kk = keys.cpu().numpy()
+    diag = (kk % dims[0]) == ((kk // dims[0]) % dims[1])
+    ref = np.bincount(kk[diag] // (dims[0] * dims[1]), weights=vals.cpu().numpy()[diag], minlength=dims[2])
+    got = np.zeros(dims[2])
+    got[ok[:m].cpu().numpy()] = ov[:m].cpu().numpy()
+    assert L.device_status() == 0 and np.allclose(got, ref, rtol=0, atol=1e-9)
+    if rank != 0:
+        return 0
+    peak, peak_kind = peaks()
+    alg = 16.0 * (n + m)
+    config = {"workload": "contract_attract b(k) = a(i,i,k): a 8192 x 8192 x 1024, 2^26 entries (a tenth on the "
+                          "diagonal), uniform, key-sorted; step = lnt_contract_attract (map, fold, scan, write)",
+              "nnz": int(n), "output_nnz": int(m), "l2": "input far larger than L2", "parallelism": "1 GPU"}
+    print(json.dumps(_line("nnz/s", n * world / (ms * 1e-3), ms, args, world, config, {
+        "gpu_launches": launches, "cpu_baseline": None, "clocks": clocks, "kernels_ms_per_step": kernels,
+        "roofline": {"bound": "hbm", "kernel": "whole contract_attract call (4 kernels + the fold)",
+                     "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (ms * 1e-3) / 1e9 / peak, "alg_bytes_per_launch": alg, "avg_launch_ms": ms,
+                     "peak_source": peak_kind, "traffic": None},
+    })), flush=True)
+    return 0
+
+
 SKEW_DIMS = (1024, 1024, 256, 256, 4096)  # a(i,j,k,l), b(k,l,m)
 
 
@@ -922,7 +1091,7 @@ def main():
     ap.add_argument("--nnz-log2", type=int, default=26,
                     help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
-    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed"],
+    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed", "outer", "unary"],
                     help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
                          "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")
     ap.add_argument("--slices", type=int, default=7, help="dense scheme I: INT8 slices per operand")
@@ -944,7 +1113,7 @@ def main():
             return 0
         return run_reference(args)
     return {"merge": run_ours, "contraction": run_contraction, "batched": run_batched,
-            "dense": run_dense, "skewed": run_skewed}[args.workload](args)
+            "dense": run_dense, "skewed": run_skewed, "outer": run_outer, "unary": run_unary}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -3,13 +3,16 @@
 //
 // collect: two kernels over tiles of 2048 pairs.
 //   lead_kernel   - one warp per tile sums the tile's leading run (the
-//                   elements before the tile's first new key) so a run that
-//                   crosses tiles is finished from per-tile summaries instead
-//                   of element by element.
-//   collect_kernel- stages the tile in shared memory, lets the thread that
-//                   holds a run's first element sum the run, counts the runs
-//                   kept, takes its output offset by decoupled look-back and
-//                   writes (key, sum) pairs contiguously.
+//                   elements before the tile's first new key; a warp tree
+//                   reduction per 32 elements) so a run that crosses tiles is
+//                   finished from per-tile summaries instead of element by
+//                   element.  Sums start from -0.0, the additive identity that
+//                   keeps the sign of an all-zero run.
+//   collect_kernel- stages the tile in shared memory, sums the runs with a
+//                   segmented reduction (per-thread sums of 8 consecutive
+//                   items, then a reverse segmented scan over the threads),
+//                   counts the runs kept, takes its output offset by decoupled
+//                   look-back and writes (key, sum) pairs contiguously.
 // Traffic: 16 B read per input pair + 16 B written per output pair.
 #include <algorithm>
 #include <cstdlib>
@@ -46,7 +49,7 @@ __global__ void __launch_bounds__(128) lead_kernel(const u64* __restrict__ keys,
     return;
   }
   const u64 prev = keys[base - 1];
-  double sum = 0.0;
+  double sum = -0.0;  // -0.0 is the additive identity that keeps the sign of zero sums
   bool anynz = false;
   bool stop = false;
   for (size_t c = base; c < end; c += 32) {
@@ -55,13 +58,11 @@ __global__ void __launch_bounds__(128) lead_kernel(const u64* __restrict__ keys,
     const u32 m = __ballot_sync(0xffffffffu, brk);  // lanes where a new key starts
     const int nvalid = (int)min((size_t)32, end - c);
     const int upto = m ? (__ffs(m) - 1) : nvalid;  // warp-uniform
-    const double v = (lane < upto) ? vals[i] : 0.0;
-    // sequential summation in index order (every lane holds the same sum)
-    for (int l = 0; l < upto; ++l) {
-      double x = __shfl_sync(0xffffffffu, v, l);
-      sum += x;
-      anynz |= (x != 0.0);
-    }
+    double v = (lane < upto) ? vals[i] : -0.0;
+    anynz |= __ballot_sync(0xffffffffu, lane < upto && v != 0.0) != 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);  // the chunk's sum, every lane
+    sum += v;
     if (m) {
       stop = true;
       break;
@@ -127,6 +128,10 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
   __shared__ u64 s_k[kPadded];
   __shared__ double s_v[kPadded];
   __shared__ u32 s_warp[kThreads / 32];
+  __shared__ double s_wsum[kThreads / 32];
+  __shared__ bool s_wnz[kThreads / 32], s_wf[kThreads / 32];
+  __shared__ double s_rsum[kThreads];
+  __shared__ bool s_rnz[kThreads], s_rf[kThreads];
   __shared__ u32 s_tile;
   __shared__ unsigned long long s_off;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -146,30 +151,96 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
   if (tid == 0) s_k[0] = base ? keys[base - 1] : 0ull;
   __syncthreads();
 
-  // ---- runs that start in this thread's items -----------------------------
+  // ---- runs: segmented sum over the tile ----------------------------------
+  // Each thread sums its kItems consecutive items: a run that ends inside the
+  // thread is finished here; the part before the thread's first head (its
+  // "lead", L) and whether it holds a head (H) feed a reverse segmented scan
+  // over the threads, R_t = L_t + (H_t ? 0 : R_{t+1}), so the thread holding
+  // a run's head adds R of the next thread to the run's open tail.  A run that
+  // reaches the tile end continues through the next tiles' lead summaries.
   u64 rk[kItems];
   double rs[kItems];
   u32 kept_mask = 0;
+  double lead_sum = -0.0, cur = -0.0;  // -0.0: the identity that keeps the sign of zero sums
+  bool lead_nz = false, cur_nz = false, seen = false;
+  int cur_j = -1;
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
-    u32 idx = tid * kItems + j;
     rk[j] = 0;
     rs[j] = 0.0;
+    const u32 idx = tid * kItems + j;
     if (idx >= tn) continue;
     const size_t gi = base + idx;
     const u64 k = s_k[pk(idx + 1)];
     const bool head = (gi == 0) || (k != s_k[pk(idx)]);
-    if (!head) continue;
-    double sum = s_v[pk(idx)];
-    bool anynz = sum != 0.0;
-    u32 m = idx + 1;
-    while (m < tn && s_k[pk(m + 1)] == k) {
-      double x = s_v[pk(m)];
-      sum += x;
-      anynz |= (x != 0.0);
-      ++m;
+    const double v = s_v[pk(idx)];
+    if (head) {
+      if (seen && (!skip_zero_heads || base + tid * kItems + cur_j == 0 || cur_nz)) {  // a run ends here
+        kept_mask |= 1u << cur_j;
+        const u64 hk = s_k[pk(tid * kItems + cur_j + 1)];
+#pragma unroll
+        for (int q = 0; q < kItems; ++q)  // static indices keep rk / rs in registers
+          if (q == cur_j) {
+            rk[q] = hk;
+            rs[q] = cur;
+          }
+      }
+      seen = true;
+      cur_j = j;
+      cur = v;
+      cur_nz = v != 0.0;
+    } else if (seen) {
+      cur += v;
+      cur_nz |= v != 0.0;
+    } else {
+      lead_sum += v;
+      lead_nz |= v != 0.0;
     }
-    if (m == tn) {  // the run may continue into later tiles
+  }
+  {  // reverse segmented scan of (L, any non-zero in L, H) over the threads
+    double rsum = lead_sum;
+    bool rnz = lead_nz, rf = seen;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double s2 = __shfl_down_sync(0xffffffffu, rsum, o);
+      const bool n2 = __shfl_down_sync(0xffffffffu, (int)rnz, o) != 0;
+      const bool f2 = __shfl_down_sync(0xffffffffu, (int)rf, o) != 0;
+      if (lane + o < 32) {
+        if (!rf) {
+          rsum += s2;
+          rnz = rnz || n2;
+        }
+        rf = rf || f2;
+      }
+    }
+    if (lane == 0) {
+      s_wsum[warp] = rsum;
+      s_wnz[warp] = rnz;
+      s_wf[warp] = rf;
+    }
+    __syncthreads();
+    double tsum = -0.0;  // the threads of the later warps
+    bool tnz = false, tf = false;
+    for (int w = kThreads / 32 - 1; w > warp; --w) {
+      tsum = s_wsum[w] + (s_wf[w] ? -0.0 : tsum);
+      tnz = s_wnz[w] || (!s_wf[w] && tnz);
+      tf = s_wf[w] || tf;
+    }
+    s_rsum[tid] = rsum + (rf ? -0.0 : tsum);
+    s_rnz[tid] = rnz || (!rf && tnz);
+    s_rf[tid] = rf || tf;
+    __syncthreads();
+  }
+  if (seen) {  // the run opened by this thread's last head
+    double sum = cur;
+    bool anynz = cur_nz;
+    bool to_end = true;
+    if (tid + 1 < kThreads) {
+      sum += s_rsum[tid + 1];
+      anynz = anynz || s_rnz[tid + 1];
+      to_end = !s_rf[tid + 1];
+    }
+    if (to_end) {  // the run may continue into later tiles
       for (u32 u = tile + 1; u < ntiles; ++u) {
         LeadSummary L = lead[u];
         sum += L.sum;
@@ -177,11 +248,16 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
         if (!L.full) break;
       }
     }
-    const bool kept = !skip_zero_heads || gi == 0 || anynz;
-    if (kept) {
-      kept_mask |= 1u << j;
-      rk[j] = k;
-      rs[j] = sum;
+    const size_t gi = base + tid * kItems + cur_j;
+    if (!skip_zero_heads || gi == 0 || anynz) {
+      kept_mask |= 1u << cur_j;
+      const u64 hk = s_k[pk(tid * kItems + cur_j + 1)];
+#pragma unroll
+      for (int q = 0; q < kItems; ++q)
+        if (q == cur_j) {
+          rk[q] = hk;
+          rs[q] = sum;
+        }
     }
   }
 

@@ -456,13 +456,35 @@ int lnt_lattice_mult(const lnt_lattice* a, const lnt_lattice* b, const void* pla
 // Products with no contracted index (SparseMIABase::perform_noLatticeMult,
 // SparseMIABase.h:1716-1826): A as a lattice (h = its outer size) x 1 x d and B
 // as 1 x wB x d (d = the inter size), both key-sorted.  Expanding every B
-// entry's products against the A entries of its tab (expand_kernel with w = 1)
-// yields them in the reference's emission order - B entries major, A entries
-// minor, tab by tab - which is ascending key order, so C needs neither a sort
-// nor a fold (equal keys from operands with duplicate keys stay separate, as
-// in the reference).
+// entry's products against the A entries of its tab (a warp per B entry, at
+// the entry's prefix-summed offset) yields them in the reference's emission
+// order - B entries major, A entries minor, tab by tab - which is ascending
+// key order, so C needs neither a sort nor a fold (equal keys from operands
+// with duplicate keys stay separate, as in the reference).
 namespace lnt {
 namespace {
+// One warp per B entry e (grid-stride): its products are the A entries of its
+// tab, written contiguously at boff[e] with coalesced reads of A and writes.
+__global__ void nolattice_expand_kernel(Lat A, Lat B, AColumns ac, const u64* __restrict__ boff, Divider div_wB,
+                                        u64* __restrict__ ck, double* __restrict__ cv) {
+  const int lane = threadIdx.x & 31;
+  const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
+  const u64 h = A.rows;
+  for (u64 e = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < B.nnz; e += nw) {
+    const u64 bk = B.keys[e];          // col + wB * tab (B has one row)
+    const u64 t = divide(bk, div_wB);
+    u64 lo, hi;
+    ac.range(t, lo, hi);
+    const double bv = B.vals[e];
+    const u64 o = boff[e];
+    const u64 shift = h * bk - t * h;  // output key = A key - t*h + h*bk
+    for (u64 x = lo + lane; x < hi; x += 32) {
+      ck[o + (x - lo)] = A.keys[x] + shift;
+      cv[o + (x - lo)] = A.vals[x] * bv;
+    }
+  }
+}
+
 struct NoLatLayout {
   size_t off_aptr, off_boff, off_scan, total;
 };
@@ -536,9 +558,8 @@ int lnt_nolattice_mult(const lnt_lattice* a, const lnt_lattice* b, uint64_t prod
   AColumns ac{s.dense_a ? reinterpret_cast<const u64*>(p + L.off_aptr) : nullptr, s.A.keys, s.A.nnz, s.h};
   {
     ProfScope prof("nolattice_expand", cs);
-    expand_kernel<<<grid_for(products, 256), 256, 0, cs>>>(s.A, s.B, ac, reinterpret_cast<const u64*>(p + L.off_boff),
-                                                          products, make_divider(s.w), make_divider(s.wB),
-                                                          (u64*)c_keys, c_vals);
+    nolattice_expand_kernel<<<grid_for(s.B.nnz * 32, 256), 256, 0, cs>>>(
+        s.A, s.B, ac, reinterpret_cast<const u64*>(p + L.off_boff), make_divider(s.wB), (u64*)c_keys, c_vals);
     count_launch();
   }
   return launch_status();
