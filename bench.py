@@ -769,8 +769,8 @@ def run_outer(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     g = torch.Generator(device=dev)
     g.manual_seed(0)
-    h, wB, d = 4096, 64, 65536
-    ak = torch.unique(torch.randint(0, h * d, (1 << 24,), generator=g, device=dev))
+    h, wB, d = 4096 >> args.shrink, 64, 65536
+    ak = torch.unique(torch.randint(0, h * d, (1 << (24 - args.shrink),), generator=g, device=dev))
     bk = torch.unique(torch.randint(0, wB * d, (1 << 21,), generator=g, device=dev))
     av = torch.rand(ak.numel(), generator=g, device=dev, dtype=torch.float64) * 2 - 1
     bv = torch.rand(bk.numel(), generator=g, device=dev, dtype=torch.float64) * 2 - 1
@@ -844,9 +844,9 @@ def run_unary(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     g = torch.Generator(device=dev)
     g.manual_seed(0)
-    dims = [8192, 8192, 1024]
+    dims = [8192, 8192, 1024 >> args.shrink]
     total = dims[0] * dims[1] * dims[2]
-    keys = torch.unique(torch.randint(0, total, (1 << 26,), generator=g, device=dev))
+    keys = torch.unique(torch.randint(0, total, (1 << (26 - args.shrink),), generator=g, device=dev))
     # a tenth of the entries on the diagonal i = i', so the output is not trivial
     idx = torch.arange(0, keys.numel(), 10, device=dev)
     i0 = keys[idx] % dims[0]
@@ -1099,6 +1099,7 @@ def main():
     ap.add_argument("--no-scheme1", action="store_true", help="dense: skip timing scheme I")
     ap.add_argument("--dense-log2", type=int, default=14, help="dense: log2 of the GEMM size (14 = the workload)")
     ap.add_argument("--skew-log2", type=int, default=25, help="skewed: log2 of coordinates drawn per operand")
+    ap.add_argument("--shrink", type=int, default=0, help="outer / unary: divide the workload by 2^shrink (profiling)")
     ap.add_argument("--skew-b-log2", type=int, default=None, help="skewed: log2 of coordinates drawn for b "
                                                                    "(default: --skew-log2)")
     ap.add_argument("--skew-dims", default=",".join(map(str, SKEW_DIMS)),
