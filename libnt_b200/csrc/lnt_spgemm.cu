@@ -478,9 +478,23 @@ __global__ void nolattice_expand_kernel(Lat A, Lat B, AColumns ac, const u64* __
     const double bv = B.vals[e];
     const u64 o = boff[e];
     const u64 shift = h * bk - t * h;  // output key = A key - t*h + h*bk
-    for (u64 x = lo + lane; x < hi; x += 32) {
-      ck[o + (x - lo)] = A.keys[x] + shift;
-      cv[o + (x - lo)] = A.vals[x] * bv;
+    for (u64 x0 = lo + lane; x0 < hi; x0 += 128) {  // four products per lane: loads first, then stores
+      u64 k[4];
+      double v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const u64 x = x0 + 32 * q;
+        k[q] = x < hi ? A.keys[x] : 0;
+        v[q] = x < hi ? A.vals[x] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const u64 x = x0 + 32 * q;
+        if (x < hi) {
+          ck[o + (x - lo)] = k[q] + shift;
+          cv[o + (x - lo)] = v[q] * bv;
+        }
+      }
     }
   }
 }
