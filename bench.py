@@ -475,7 +475,68 @@ def run_contraction(args):
         step(True)
     f1.record()
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+    e2e_eager_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+
+    # The same step as one CUDA graph: C-ABI calls on buffers sized from the
+    # warm-up (the product count and output capacity of a fixed-shape
+    # contraction), no host synchronisation inside; e2e adds the host copies.
+    import ctypes as C
+    lib = L.lib()
+    A = L.Lattice.of(sa[0], sa[1], 100, 10 ** 4, 1)
+    B = L.Lattice.of(sb[0], sb[1], 10 ** 4, 100, 1)
+    nb_ = C.c_size_t(0)
+    L._check(lib.lnt_lattice_mult_plan_workspace(C.byref(A), C.byref(B), C.byref(nb_)), "plan_workspace")
+    plan = L.workspace(nb_.value, dev)
+    L._check(lib.lnt_lattice_mult_workspace(C.byref(A), C.byref(B), C.c_uint64(prods), C.byref(nb_)), "workspace")
+    mws = L.workspace(nb_.value, dev)
+    counts = torch.zeros(2, dtype=torch.int64, device=dev)
+    cap = 100 * 100
+    gk = torch.empty(cap, dtype=torch.int64, device=dev)
+    gv = torch.empty(cap, dtype=torch.float64, device=dev)
+    gn = torch.zeros(1, dtype=torch.int64, device=dev)
+    hn = torch.zeros(1, dtype=torch.int64, pin_memory=True)
+
+    def graph_step(host_io):
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        if host_io:
+            for d_, h_ in zip(dk, hk):
+                d_.copy_(h_, non_blocking=True)
+        L.permute_sort(dk[0], dk[1], max_key=10 ** 6, rekey=spec_a, out_keys=sa[0], out_vals=sa[1], ws=ws)
+        L.permute_sort(dk[2], dk[3], max_key=10 ** 6, rekey=spec_b, out_keys=sb[0], out_vals=sb[1], ws=ws)
+        L._check(lib.lnt_lattice_mult_plan(C.byref(A), C.byref(B), C.c_void_p(plan.data_ptr()), plan.numel(),
+                                           C.c_void_p(counts.data_ptr()), st), "plan")
+        L._check(lib.lnt_lattice_mult(C.byref(A), C.byref(B), C.c_void_p(plan.data_ptr()), C.c_uint64(prods),
+                                      C.c_void_p(mws.data_ptr()), mws.numel(), C.c_void_p(gk.data_ptr()),
+                                      C.c_void_p(gv.data_ptr()), C.c_void_p(gn.data_ptr()), st), "mult")
+        if host_io:
+            out_h[0][:nc].copy_(gk[:nc], non_blocking=True)
+            out_h[1][:nc].copy_(gv[:nc], non_blocking=True)
+            hn.copy_(gn, non_blocking=True)
+
+    graph_ms, e2e_graph_ms = {}, {}
+    for host_io, res in ((False, graph_ms), (True, e2e_graph_ms)):
+        graph_step(host_io)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            graph_step(host_io)
+        for _ in range(args.warmup):
+            g.replay()
+        torch.cuda.synchronize()
+        h0, h1 = _events()
+        h0.record()
+        for _ in range(args.steps):
+            g.replay()
+        h1.record()
+        torch.cuda.synchronize()
+        res["ms"] = max_over_ranks(h0.elapsed_time(h1) / args.steps, world)
+        del g
+    assert int(gn.item()) == nc and L.device_status() == 0
+    ck_e, _, _ = L.lattice_mult(sa[0], sa[1], sb[0], sb[1], 100, 10 ** 4, 100, 1)
+    assert torch.equal(ck_e, gk[:nc])
+    eager_ms = ms
+    ms = graph_ms["ms"]
+    e2e_ms = e2e_graph_ms["ms"]
     if rank != 0:
         return 0
     cpu = None
@@ -498,8 +559,10 @@ def run_contraction(args):
                "kind": "reference" if oracle.ref_available() else "port",
                "sample": "the full workload, median-free mean of 20 runs: reference sorts + restated csc_no_accum"}
     config = {"workload": "plain sparse contraction c(i,l)=a(i,j,k)*b(k,l,j), dims 100^3, 10^4 nnz each, "
-                          "seed 0, both unsorted (sort a, re-key+sort b, csc_no_accum)",
-              "products": prods, "output_nnz": nc, "l2": "inputs fit in L2 (latency-bound workload)"}
+                          "seed 0, both unsorted (sort a, re-key+sort b, csc_no_accum); a step = one CUDA-graph "
+                          "replay of that sequence of C-ABI calls",
+              "products": prods, "output_nnz": nc, "l2": "inputs fit in L2 (latency-bound workload)",
+              "eager_ms_per_step": eager_ms, "eager_e2e_ms_per_step": e2e_eager_ms}
     print(json.dumps(_line("products/s", prods * world / (ms * 1e-3), ms, args, world, config, {
         "e2e": {"value": prods * world / (e2e_ms * 1e-3), "unit": "products/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 4 * 8 * 10 ** 4, "d2h_bytes_per_step": 16 * nc + 16},
