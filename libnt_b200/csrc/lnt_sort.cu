@@ -261,7 +261,35 @@ __global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>:
     }
   }
 
+  __syncthreads();  // the per-(warp, digit) bases are complete
+  // ---- stable rank: ballot match + per-(warp, digit) running base ---------
+  u32 pos[ITEMS];
+  const u32 lt_mask = (1u << lane) - 1u;
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const u32 off = warp_base + i * 32 + lane;
+    const bool valid = off < tile_n;
+    const u32 vmask = __ballot_sync(0xffffffffu, valid);
+    const u32 d = valid ? ((u32)(key[i] >> shift) & mask) : 0u;
+    const u32 peers = match_digit<BITS>(d) & vmask;
+    u32 base = 0;
+    if (valid) base = s_whist[warp * RADIX + d];
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) s_whist[warp * RADIX + d] = base + __popc(peers);
+    __syncwarp();
+    pos[i] = base + __popc(peers & lt_mask);
+  }
+  // ---- stage keys in digit order ------------------------------------------
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const u32 off = warp_base + i * 32 + lane;
+    if (off < tile_n) s_x[pos[i]] = key[i];
+  }
+  __syncthreads();
+
   // ---- decoupled look-back, W predecessors per round trip per digit -------
+  // (after the local ranking: predecessors have had that long to publish
+  // their inclusive prefixes, so the walk back is shorter)
   {
     u32 excl[DPT];
     int p[DPT];
@@ -321,31 +349,6 @@ __global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>:
       if (tile != 0) st_volatile(&status[(size_t)tile * RADIX + d], kFlagPre | (excl[j] + cnt[j]));
       s_glob[d] = excl[j] - tstart[j];
     }
-  }
-  __syncthreads();
-
-  // ---- stable rank: ballot match + per-(warp, digit) running base ---------
-  u32 pos[ITEMS];
-  const u32 lt_mask = (1u << lane) - 1u;
-#pragma unroll
-  for (int i = 0; i < ITEMS; ++i) {
-    const u32 off = warp_base + i * 32 + lane;
-    const bool valid = off < tile_n;
-    const u32 vmask = __ballot_sync(0xffffffffu, valid);
-    const u32 d = valid ? ((u32)(key[i] >> shift) & mask) : 0u;
-    const u32 peers = match_digit<BITS>(d) & vmask;
-    u32 base = 0;
-    if (valid) base = s_whist[warp * RADIX + d];
-    __syncwarp();
-    if (valid && lane == __ffs(peers) - 1) s_whist[warp * RADIX + d] = base + __popc(peers);
-    __syncwarp();
-    pos[i] = base + __popc(peers & lt_mask);
-  }
-  // ---- stage keys in digit order ------------------------------------------
-#pragma unroll
-  for (int i = 0; i < ITEMS; ++i) {
-    const u32 off = warp_base + i * 32 + lane;
-    if (off < tile_n) s_x[pos[i]] = key[i];
   }
   __syncthreads();
 

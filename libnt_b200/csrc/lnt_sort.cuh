@@ -4,10 +4,11 @@
 //      the last block to finish turns them into exclusive bin starts.
 //   2. per pass, onesweep_kernel: each CTA takes the next tile id, counts its
 //      tile's digits and publishes them at once, starts the value copy into
-//      shared memory (cp.async), obtains its global digit offsets by a
-//      windowed decoupled look-back over predecessor tiles, ranks its keys
-//      stably (warp ballots + per-warp counters), reorders keys and values in
-//      shared memory by digit and writes them out in digit runs.
+//      shared memory (cp.async), ranks its keys stably (warp ballots +
+//      per-warp counters) and stages them in digit order, then obtains its
+//      global digit offsets by a windowed decoupled look-back over
+//      predecessor tiles (after the ranking, so predecessors have had time to
+//      publish inclusive prefixes) and writes keys and values in digit runs.
 // Traffic per pass: 16 B read + 16 B written per pair (the HBM roofline).
 // The first pass reads through a PairSource, which concatenates two arrays
 // and re-keys each on the fly, so sortMerge's re-key + concatenation costs
