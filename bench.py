@@ -40,8 +40,9 @@ MAX_KEY = 512 ** 4
 INDEX_ORDER = [3, 2, 1, 0]  # c(i,j,k,l) = a(i,j,k,l) + b(l,k,j,i)
 WORKLOAD = ("sparse merge c(i,j,k,l)=a(i,j,k,l)+b(l,k,j,i): order-4 SparseMIA dims 512^4, "
             "2^26 nnz per operand, uniform coordinates, f64 values U[-1,1], both unsorted (sortMerge: "
-            "re-key A to {3,2,1,0}, concatenate, radix-sort the 2^27 (u64,f64) pairs, collect duplicates; here a "
-            "bucket histogram, two 8-bit onesweep passes and a per-bucket shared-memory sort with the fold fused)")
+            "re-key A to {3,2,1,0}, concatenate, radix-sort the 2^27 (u64,f64) pairs, collect duplicates)")
+IMPLEMENTATION = ("bucket histogram (A re-keyed on the fly), two 8-bit onesweep passes over the top 15 key bits, "
+                  "per-bucket shared-memory sort with the duplicate fold fused")
 HBM_FALLBACK_GBS = 6650.0
 
 
@@ -381,7 +382,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "nnz/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nnz_per_operand": NNZ, "output_nnz": n_out,
+            "config": {"workload": WORKLOAD, "implementation": IMPLEMENTATION, "nnz_per_operand": NNZ, "output_nnz": n_out,
                        "l2": "inputs (2 GiB) and sort buffers larger than the 126 MB L2; no flush needed",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "nnz/s", "ms_per_step": e2e_ms,
