@@ -966,6 +966,62 @@ def run_unary(args):
     return 0
 
 
+def run_scanmerge(args):
+    """The merge workload with both operands already sorted (each under its
+    default sequence): perform_outside_merge sorts A into B's order (sort(seq):
+    re-key {0,1,2,3} -> {3,2,1,0} + sort) and merges linearly.  A step =
+    lnt_permute_sort(A) + lnt_merge_sorted(A', B) through the C ABI."""
+    import ctypes as C
+
+    import torch
+
+    import libnt_b200 as L
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    n = 1 << args.nnz_log2
+    ak = torch.sort(torch.randint(0, MAX_KEY, (n,), generator=g, device=dev)).values
+    bk = torch.sort(torch.randint(0, MAX_KEY, (n,), generator=g, device=dev)).values
+    av = torch.rand(n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    bv = torch.rand(n, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    spec = L.RekeySpec.make(DIMS, [0, 1, 2, 3], [3, 2, 1, 0])
+    sk, sv = torch.empty_like(ak), torch.empty_like(av)
+    ws_s = L.workspace(L.permute_sort_workspace(n, MAX_KEY), dev)
+    lib = L.lib()
+    nb_ = C.c_size_t(0)
+    L._check(lib.lnt_merge_sorted_workspace(n, n, C.byref(nb_)), "merge workspace")
+    ws_m = L.workspace(nb_.value, dev)
+    ok = torch.empty(2 * n, dtype=torch.int64, device=dev)
+    ov = torch.empty(2 * n, dtype=torch.float64, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    def step():
+        L.permute_sort(ak, av, max_key=MAX_KEY, rekey=spec, out_keys=sk, out_vals=sv, ws=ws_s)
+        L.merge_sorted(sk, sv, bk, bv, 0, out_keys=ok, out_vals=ov, count=cnt, ws=ws_m, sync=False)
+
+    ms, launches, clocks = _timed_steps(torch, step, args)
+    kernels = {k: L.profile_query(k)[0] / args.steps for k in ("sort_hist", "sort_onesweep", "merge")}
+    ms = max_over_ranks(ms, world)
+    m = int(cnt.item())
+    assert L.device_status() == 0 and bool(torch.all(ok[1:m] >= ok[:m - 1]).item())  # duplicates within an operand stay
+    if rank != 0:
+        return 0
+    peak, peak_kind = peaks()
+    mg = kernels["merge"]
+    alg = 32.0 * n + 16.0 * m
+    config = {"workload": "sparse merge c(i,j,k,l)=a(i,j,k,l)+b(l,k,j,i), 512^4, 2^%d nnz per operand, both "
+                          "operands sorted (outside_scanMerge: sort(seq) of a into b's order, linear merge)"
+                          % args.nnz_log2, "output_nnz": m, "l2": "inputs larger than L2", "parallelism": "1 GPU"}
+    print(json.dumps(_line("nnz/s", 2 * n * world / (ms * 1e-3), ms, args, world, config, {
+        "gpu_launches": launches, "kernels_ms_per_step": kernels, "cpu_baseline": None, "clocks": clocks,
+        "roofline": {"bound": "hbm", "kernel": "merge_kernel (the linear merge)", "achieved": alg / (mg * 1e-3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": alg / (mg * 1e-3) / 1e9 / peak,
+                     "alg_bytes_per_launch": alg, "avg_launch_ms": mg, "peak_source": peak_kind, "traffic": None},
+    })), flush=True)
+    return 0
+
+
 SKEW_DIMS = (1024, 1024, 256, 256, 4096)  # a(i,j,k,l), b(k,l,m)
 
 
@@ -1155,7 +1211,7 @@ def main():
     ap.add_argument("--nnz-log2", type=int, default=26,
                     help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
-    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed", "outer", "unary"],
+    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed", "outer", "unary", "scanmerge"],
                     help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
                          "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")
     ap.add_argument("--slices", type=int, default=7, help="dense scheme I: INT8 slices per operand")
@@ -1178,7 +1234,8 @@ def main():
             return 0
         return run_reference(args)
     return {"merge": run_ours, "contraction": run_contraction, "batched": run_batched,
-            "dense": run_dense, "skewed": run_skewed, "outer": run_outer, "unary": run_unary}[args.workload](args)
+            "dense": run_dense, "skewed": run_skewed, "outer": run_outer, "unary": run_unary,
+            "scanmerge": run_scanmerge}[args.workload](args)
 
 
 if __name__ == "__main__":
