@@ -17,9 +17,13 @@
 //   B_i with key k: ubA = (merged position) - i is one past the last A with
 //     key k; j = occurrence of k in B up to i; B_i is consumed iff
 //     A[ubA - 1 - j] has key k.
-// Emitted elements keep merged order; their output offsets come from a block
-// scan plus a decoupled look-back over tiles.  Traffic: 16 B read per input
-// pair + 16 B written per output pair (+ neighbour reads that hit in cache).
+// A partition kernel finds every tile's split first (one merge-path search per
+// tile boundary, all in parallel); each tile then stages its A and B slices
+// (keys and values) in shared memory with coalesced loads, and run indices and
+// partners are read from there - global memory only when a run of equal keys
+// crosses the slice boundary.  Emitted elements keep merged order; their output
+// offsets come from a block scan plus a decoupled look-back over tiles.
+// Traffic: 16 B read per input pair + 16 B written per output pair.
 #include <algorithm>
 
 #include "lnt_sort.cuh"
@@ -73,17 +77,25 @@ __device__ __forceinline__ size_t run_index(const u64* __restrict__ x, size_t i,
 
 __device__ __forceinline__ double apply_op(int op, double a, double b) { return op == 0 ? a + b : a - b; }
 
+// splits[t] = A elements among the first min(t * kTile, na + nb) of the merge.
+__global__ void merge_partition_kernel(const u64* __restrict__ a, size_t na, const u64* __restrict__ b, size_t nb,
+                                       u32 ntiles, u64* __restrict__ splits) {
+  const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > ntiles) return;
+  splits[t] = merge_path(a, na, b, nb, min(na + nb, (size_t)t * kTile));
+}
+
 __global__ void __launch_bounds__(kThreads) merge_kernel(const u64* __restrict__ ak, const double* __restrict__ av,
                                                          size_t na, const u64* __restrict__ bk,
                                                          const double* __restrict__ bv, size_t nb, int op,
-                                                         u32 ntiles, unsigned long long* __restrict__ status,
+                                                         u32 ntiles, const u64* __restrict__ splits,
+                                                         unsigned long long* __restrict__ status,
                                                          u32* __restrict__ tile_counter, u64* __restrict__ ck,
                                                          double* __restrict__ cv, u64* __restrict__ d_nout) {
   __shared__ u64 s_k[kTile];
   __shared__ double s_v[kTile];
   __shared__ u32 s_warp[kThreads / 32];
   __shared__ u32 s_tile;
-  __shared__ unsigned long long s_split[2];
   __shared__ unsigned long long s_off;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -92,14 +104,19 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const u64* __restrict__
   const size_t total = na + nb;
   const size_t d0 = (size_t)tile * kTile;
   const size_t d1 = min(total, d0 + kTile);
-  if (tid < 2) s_split[tid] = merge_path(ak, na, bk, nb, tid == 0 ? d0 : d1);
-  __syncthreads();
-  const size_t a0 = s_split[0], a1 = s_split[1];
+  const size_t a0 = splits[tile], a1 = splits[tile + 1];
   const size_t b0 = d0 - a0, b1 = d1 - a1;
   const int la = (int)(a1 - a0), lb = (int)(b1 - b0);
-  // stage the tile's A slice then its B slice in shared memory (keys only; values
-  // are fetched per output below)
-  for (int i = tid; i < la + lb; i += kThreads) s_k[i] = i < la ? ak[a0 + i] : bk[b0 + (i - la)];
+  // stage the tile's A slice then its B slice, keys and values, in shared memory
+  for (int i = tid; i < la + lb; i += kThreads) {
+    if (i < la) {
+      s_k[i] = __ldcs(ak + a0 + i);
+      s_v[i] = __ldcs(av + a0 + i);
+    } else {
+      s_k[i] = __ldcs(bk + b0 + (i - la));
+      s_v[i] = __ldcs(bv + b0 + (i - la));
+    }
+  }
   __syncthreads();
   // each thread merges kItems consecutive merged positions
   const int dt = min(tid * kItems, la + lb);
@@ -122,9 +139,16 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const u64* __restrict__
       const size_t i = a0 + ia;
       const u64 k = s_k[ia];
       const size_t lbB = mg - i;  // B elements before A_i: those with key < k
-      const size_t j = run_index(ak, i, k);
-      double v = av[i];
-      if (lbB + j < nb && bk[lbB + j] == k) v = apply_op(op, v, bv[lbB + j]);
+      size_t j = 0;               // occurrence of k in A before A_i
+      while ((int)j < ia && s_k[ia - 1 - j] == k) ++j;
+      if ((int)j == ia) j += run_index(ak, a0, k);
+      double v = s_v[ia];
+      const size_t pb = lbB + j;  // the partner B, if it has key k
+      if (pb >= b0 && pb < b1) {
+        if (s_k[la + (int)(pb - b0)] == k) v = apply_op(op, v, s_v[la + (int)(pb - b0)]);
+      } else if (pb < nb && bk[pb] == k) {
+        v = apply_op(op, v, bv[pb]);
+      }
       emit[q] = true;
       ek[q] = k;
       evv[q] = v;
@@ -133,12 +157,18 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const u64* __restrict__
       const size_t i = b0 + ib;
       const u64 k = s_k[la + ib];
       const size_t ubA = mg - i;  // A elements before B_i: those with key <= k
-      const size_t j = run_index(bk, i, k);
-      const bool consumed = ubA >= j + 1 && ak[ubA - 1 - j] == k;
+      size_t j = 0;               // occurrence of k in B before B_i
+      while ((int)j < ib && s_k[la + ib - 1 - j] == k) ++j;
+      if ((int)j == ib) j += run_index(bk, b0, k);
+      bool consumed = false;
+      if (ubA >= j + 1) {
+        const size_t pa = ubA - 1 - j;  // the A it would pair with
+        consumed = (pa >= a0 && pa < a1) ? s_k[(int)(pa - a0)] == k : ak[pa] == k;
+      }
       if (!consumed) {
         emit[q] = true;
         ek[q] = k;
-        evv[q] = apply_op(op, 0.0, bv[i]);
+        evv[q] = apply_op(op, 0.0, s_v[la + ib]);
       }
       ++ib;
     }
@@ -215,7 +245,7 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const u64* __restrict__
 
 struct MergeLayout {
   u32 ntiles;
-  size_t off_status, off_counter, total;
+  size_t off_status, off_counter, off_splits, total;
 };
 
 static MergeLayout merge_layout(size_t n) {
@@ -223,7 +253,8 @@ static MergeLayout merge_layout(size_t n) {
   L.ntiles = (u32)((n + kTile - 1) / kTile);
   L.off_status = 0;
   L.off_counter = align_up((size_t)std::max<u32>(L.ntiles, 1) * 8, 256);
-  L.total = L.off_counter + 256;
+  L.off_splits = L.off_counter + 256;
+  L.total = L.off_splits + align_up(((size_t)L.ntiles + 1) * 8, 256);
   return L;
 }
 
@@ -270,16 +301,19 @@ int lnt_merge_sorted(const uint64_t* a_keys, const double* a_vals, size_t na, co
   if (!c_keys || !c_vals) return LNT_BAD_ARG;
   MergeLayout L = merge_layout(n);
   if (!workspace || workspace_bytes < L.total) return LNT_WORKSPACE;
-  if (cudaMemsetAsync(workspace, 0, L.total, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  if (cudaMemsetAsync(workspace, 0, L.off_splits, s) != cudaSuccess) return LNT_DEVICE_ERROR;
   unsigned char* w = static_cast<unsigned char*>(workspace);
+  u64* splits = reinterpret_cast<u64*>(w + L.off_splits);
   {
     ProfScope prof("merge", s);
+    merge_partition_kernel<<<(L.ntiles + 1 + 255) / 256, 256, 0, s>>>((const u64*)a_keys, na, (const u64*)b_keys, nb,
+                                                                       L.ntiles, splits);
     merge_kernel<<<L.ntiles, kThreads, 0, s>>>((const u64*)a_keys, a_vals, na, (const u64*)b_keys, b_vals, nb, op,
-                                               L.ntiles, reinterpret_cast<unsigned long long*>(w + L.off_status),
+                                               L.ntiles, splits, reinterpret_cast<unsigned long long*>(w + L.off_status),
                                                reinterpret_cast<u32*>(w + L.off_counter), (u64*)c_keys, c_vals,
                                                (u64*)d_nout);
   }
-  count_launch();
+  count_launch(2);
   return launch_status();
 }
 
