@@ -253,6 +253,35 @@ LNT_API int lnt_nolattice_mult_count(const lnt_lattice* A, const lnt_lattice* B,
 LNT_API int lnt_nolattice_mult(const lnt_lattice* A, const lnt_lattice* B, uint64_t products, void* workspace,
                                size_t workspace_bytes, uint64_t* c_keys, double* c_vals, void* stream);
 
+/* Mixed sparse / dense lattice products: the mex gateway
+ * SparseDenseLatticeMultMex(a_vals, a_idx, a_dims, B, dense_first)
+ * (MATLAB/mex/sparse_denselattice_mul.cpp:8-106).  S is the sparse operand,
+ * D the dense one (float64 column-major, tabs one after another), `other` the
+ * dense operand's extent that S does not share.  Every non-empty line of S
+ * gives a full dense line of C (h or wB entries, exact zeros kept); each
+ * entry is sum over the line's entries (k, v) of S, in key order, of
+ * v * D(...), accumulated from 0 as c = c + v * d (no fused multiply-add).
+ *   dense_first = 1: C = A * S, DenseLatticeBase::operator*(SparseLatticeBase)
+ *     (DenseLatticeBase.h:436-500).  A is other x rows(S) x tabs(S); S keys
+ *     sorted column-major (row + rows (col + cols tab)); C is other x cols(S)
+ *     x tabs(S) with column-major keys i + other (col + cols tab), ascending.
+ *   dense_first = 0: C = S * B, SparseLatticeBase::operator*(DenseLatticeBase)
+ *     (SparseLatticeBase.h:1148-1162, evaluated as (B^T S^T)^T).  S keys sorted
+ *     ROW-major (col + cols (row + rows tab), the order that product leaves its
+ *     operand in); B is cols(S) x other x tabs(S); C is rows(S) x other x
+ *     tabs(S) with the reference's row-major lattice keys
+ *     j + other (row + rows tab), ascending.
+ * Two phases sharing one workspace: lnt_sparse_dense_mult_count finds the
+ * lines of S and writes the output count to *d_count; lnt_sparse_dense_mult
+ * writes C.  Keys must lie below rows * cols * tabs (entries past the last
+ * tab contribute nothing).  LNT_BAD_DIMS for non-positive extents. */
+LNT_API int lnt_sparse_dense_mult_workspace(const lnt_lattice* S, int64_t other, int dense_first, size_t* bytes);
+LNT_API int lnt_sparse_dense_mult_count(const lnt_lattice* S, int64_t other, int dense_first, void* workspace,
+                                        size_t workspace_bytes, uint64_t* d_count, void* stream);
+LNT_API int lnt_sparse_dense_mult(const double* D, const lnt_lattice* S, int64_t other, int dense_first,
+                                  void* workspace, size_t workspace_bytes, uint64_t* c_keys, double* c_vals,
+                                  void* stream);
+
 /* Unary contraction / attraction: SparseMIABase::contract_attract
  * (SparseMIABase.h:1913-2053), which MIA_Atom applies to index labels repeated
  * inside one operand (perform_unary, MIA_Expr.h:690-735).  keys/vals: the

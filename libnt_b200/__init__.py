@@ -95,6 +95,9 @@ _SIGS = {
     "lnt_nolattice_mult_workspace": ([C.POINTER(Lattice), C.POINTER(Lattice), C.POINTER(C.c_size_t)], C.c_int),
     "lnt_nolattice_mult_count": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, _sz, _vp, _vp], C.c_int),
     "lnt_nolattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), C.c_uint64, _vp, _sz, _vp, _vp, _vp], C.c_int),
+    "lnt_sparse_dense_mult_workspace": ([C.POINTER(Lattice), C.c_int64, C.c_int, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_sparse_dense_mult_count": ([C.POINTER(Lattice), C.c_int64, C.c_int, _vp, _sz, _vp, _vp], C.c_int),
+    "lnt_sparse_dense_mult": ([_vp, C.POINTER(Lattice), C.c_int64, C.c_int, _vp, _sz, _vp, _vp, _vp], C.c_int),
     "lnt_batched_workspace": ([C.c_int, _vp, _vp, _vp, C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)], C.c_int),
     "lnt_batched_prepare": ([C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
     "lnt_batched_lattice_mult": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp], C.c_int),
@@ -375,6 +378,33 @@ def nolattice_mult(a_keys, a_vals, b_keys, b_vals, h: int, wB: int, d: int = 1):
     cv = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
     _check(lib().lnt_nolattice_mult(C.byref(A), C.byref(B), n, _ptr(ws), ws.numel(), _ptr(ck), _ptr(cv), _stream()),
            "lnt_nolattice_mult")
+    return ck[:n], cv[:n]
+
+
+def sparse_dense_mult(dense, s_keys, s_vals, rows: int, cols: int, tabs: int, other: int, dense_first: bool):
+    """Mixed lattice product (SparseDenseLatticeMultMex).  dense_first: C = A * S
+    with A (other x rows x tabs) and S column-major key-sorted; else C = S * B
+    with S row-major key-sorted (col + cols (row + rows tab)) and B (cols x
+    other x tabs).  dense: float64 column-major device tensor.  Returns (keys,
+    vals) of C, ascending (column-major keys for dense_first, row-major
+    lattice keys otherwise)."""
+    torch = _torch()
+    _dev(dense)
+    S = Lattice.of(s_keys, s_vals, rows, cols, tabs)
+    dev = s_keys.device
+    df = 1 if dense_first else 0
+    b = C.c_size_t(0)
+    _check(lib().lnt_sparse_dense_mult_workspace(C.byref(S), other, df, C.byref(b)),
+           "lnt_sparse_dense_mult_workspace")
+    ws = workspace(b.value, dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    _check(lib().lnt_sparse_dense_mult_count(C.byref(S), other, df, _ptr(ws), ws.numel(), _ptr(cnt), _stream()),
+           "lnt_sparse_dense_mult_count")
+    n = int(cnt.item())
+    ck = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    cv = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+    _check(lib().lnt_sparse_dense_mult(_ptr(dense), C.byref(S), other, df, _ptr(ws), ws.numel(), _ptr(ck), _ptr(cv),
+                                       _stream()), "lnt_sparse_dense_mult")
     return ck[:n], cv[:n]
 
 

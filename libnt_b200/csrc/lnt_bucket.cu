@@ -10,9 +10,11 @@
 //      group the pairs by bucket; the first reads through the PairSource
 //      (re-key + concatenation fused);
 //   3. bucket_sort_collect_kernel: one CTA per bucket (at most 5120 pairs)
-//      sorts the remaining low bits entirely in shared memory (7-bit local
-//      passes over packed (low key << 13 | local index) words; values stay put
-//      and are gathered once), folds runs of equal keys (equal keys share
+//      sorts the remaining low bits entirely in shared memory: packed (low
+//      key << 13 | local index) words are counted into 4096 sub-buckets,
+//      placed, and ranked within their sub-bucket (7-bit local LSD passes
+//      instead when a sub-bucket holds more than 32 words); values stay put
+//      and are gathered once.  It folds runs of equal keys (equal keys share
 //      their bucket) with the collect_duplicates rule, takes its output offset
 //      by decoupled look-back over buckets and writes the result once.
 // DRAM traffic: 8 B (histogram) + 2 x 32 B (passes) + 16 B + 16 B per pair
@@ -169,7 +171,7 @@ __device__ __forceinline__ u32 slot(u32 p) { return p + (p >> 5); }
 constexpr int kSlots = kBCap + kBCap / 32;
 
 constexpr int kSubBits = 12;              // counting pass over the top 12 low bits
-constexpr int kSubMax = 32;               // largest sub-bucket the insertion sort takes
+constexpr int kSubMax = 32;               // largest sub-bucket ranked by counting
 
 struct BucketSmem {
   static constexpr size_t bytes =
@@ -214,9 +216,9 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
 
   // ---- counting pass over the top sub-bucket bits ----------------------------
   // Shared atomics hand out a slot inside each sub-bucket; a block scan of the
-  // sub-bucket counts places every word; one thread then insertion-sorts each
-  // (tiny) sub-bucket by the whole packed word, i.e. by key and then by input
-  // index, so the result is the stable order.
+  // sub-bucket counts places every word; each word then finds its rank among
+  // the (few) words of its sub-bucket by the whole packed word, i.e. by key
+  // and then by input index, so the result is the stable order.
   const int sb_bits = min(low_bits, kSubBits);
   const int nsb = 1 << sb_bits;
   const int sb_shift = kIdxBits + low_bits - sb_bits;
@@ -270,24 +272,33 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
   }
   const bool small_subs = s_misc[1] <= (u32)kSubMax;
   if (small_subs) {
+    // place each word in its sub-bucket, then rank it among the (few) words of
+    // its sub-bucket: every thread ranks its own words, with no serial pass
 #pragma unroll
     for (int i = 0; i < kBItems; ++i) {
       const u32 p = warp_base + i * 32 + lane;
       if (p < cnt) s_x[slot(s_sub[(u32)(w[i] >> sb_shift) & (u32)(nsb - 1)] + rnk[i])] = w[i];
     }
     __syncthreads();
-    for (int x = tid; x < nsb; x += kBT) {
-      const u32 lo = s_sub[x], hi = x + 1 < nsb ? s_sub[x + 1] : cnt;
-      for (u32 a = lo + 1; a < hi; ++a) {  // insertion sort of a few words
-        const u64 v = s_x[slot(a)];
-        u32 z = a;
-        while (z > lo && s_x[slot(z - 1)] > v) {
-          s_x[slot(z)] = s_x[slot(z - 1)];
-          --z;
+#pragma unroll
+    for (int i = 0; i < kBItems; ++i) {  // rnk[i] becomes the final position, or ~0 if already there
+      const u32 p = warp_base + i * 32 + lane;
+      u32 fin = ~0u;
+      if (p < cnt) {
+        const u32 sb = (u32)(w[i] >> sb_shift) & (u32)(nsb - 1);
+        const u32 lo = s_sub[sb], hi = sb + 1 < (u32)nsb ? s_sub[sb + 1] : cnt;
+        if (hi - lo > 1) {
+          u32 r = 0;
+          for (u32 q = lo; q < hi; ++q) r += s_x[slot(q)] < w[i] ? 1u : 0u;
+          fin = lo + r;
         }
-        s_x[slot(z)] = v;
       }
+      rnk[i] = fin;
     }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kBItems; ++i)
+      if (rnk[i] != ~0u) s_x[slot(rnk[i])] = w[i];
     __syncthreads();
   } else {
   // ---- clustered keys: local LSD passes over the low bits -----------------------

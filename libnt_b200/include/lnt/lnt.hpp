@@ -818,6 +818,117 @@ inline DenseExpr operator*(DenseAtom a, DenseAtom b) {
   return {std::move(c), std::move(labels)};
 }
 
+// ---- mixed sparse / dense products ---------------------------------------------
+// MIA_Atom::operator* with one sparse and one dense operand (MIA_Expr.h:
+// 864-925): the sparse operand becomes a sorted lattice, the dense one a
+// zero-copy lattice (DenseMIA::toStraightLattice, DenseMIA.h:1240-1255; modes
+// already in lattice order), and the lattice product is the mixed one
+// (SparseDenseLatticeMultMex).  The result is sparse with dims [left outer,
+// right outer, inter]: every non-empty line of the sparse operand gives a full
+// line of it.
+namespace detail {
+
+inline bool lattice_ordered(const std::vector<int>& x, const std::vector<int>& y, const std::vector<int>& z) {
+  std::vector<int> s = x;
+  s.insert(s.end(), y.begin(), y.end());
+  s.insert(s.end(), z.begin(), z.end());
+  for (size_t i = 0; i < s.size(); ++i)
+    if (s[i] != (int)i) return false;
+  return true;
+}
+
+inline int64_t dense_prod(const DenseTensor& t, const std::vector<int>& m) {
+  int64_t p = 1;
+  for (int i : m) p *= t.dim(i);
+  return p;
+}
+
+// S keyed as a lattice (column-major for dense_first, row-major otherwise)
+inline void mixed_mult(const double* D, const lnt_lattice& S, int64_t other, int dense_first,
+                       DeviceBuffer<uint64_t>& k, DeviceBuffer<double>& v) {
+  size_t need = 0;
+  check(lnt_sparse_dense_mult_workspace(&S, other, dense_first, &need), "mixed product");
+  void* ws = scratch(need);
+  DeviceBuffer<uint64_t> cnt(1);
+  check(lnt_sparse_dense_mult_count(&S, other, dense_first, ws, need, cnt.data(), nullptr), "mixed product");
+  const uint64_t n = read_u64(cnt.data());
+  k = DeviceBuffer<uint64_t>(std::max<uint64_t>(n, 1));
+  v = DeviceBuffer<double>(std::max<uint64_t>(n, 1));
+  check(lnt_sparse_dense_mult(D, &S, other, dense_first, ws, need, k.data(), v.data(), nullptr), "mixed product");
+  k.shrink(n);
+  v.shrink(n);
+}
+
+}  // namespace detail
+
+// SparseMIA * DenseMIA: SparseLatticeBase::operator*(DenseLatticeBase)
+// (SparseLatticeBase.h:1148-1162).  The sparse operand is left sorted under
+// [inner, outer, inter] (the row-major lattice order that product sorts it
+// into), flagged unsorted; the result is re-keyed from the row-major lattice
+// to the default sequence and flagged unsorted, as SparseMIA(dims,
+// SparseLattice&&) does with a row-major lattice (SparseMIA.h:362-372).
+inline SparseExpr operator*(SparseAtom a, DenseAtom b) {
+  const detail::ProductOrders o = detail::product_orders(a.labels, b.labels);
+  if (o.l_inner.empty()) throw MIAParameterException("a sparse x dense product needs a contracted index");
+  if (!detail::lattice_ordered(o.r_inner, o.r_outer, o.r_inter))
+    throw MIAParameterException("the dense operand needs its modes already in lattice order");
+  const int64_t h = (int64_t)detail::prod_dims(*a.m, o.l_outer), w = (int64_t)detail::prod_dims(*a.m, o.l_inner);
+  const int64_t d = (int64_t)detail::prod_dims(*a.m, o.l_inter), wB = detail::dense_prod(*b.m, o.r_outer);
+  if (detail::dense_prod(*b.m, o.r_inner) != w || detail::dense_prod(*b.m, o.r_inter) != d)
+    throw DimensionMismatchException("mixed product dims");
+  detail::to_lattice(*a.m, o.l_inner, o.l_outer, o.l_inter);
+  const lnt_lattice S{a.m->keys(), a.m->vals(), a.m->size(), h, w, d};
+  DeviceBuffer<uint64_t> k;
+  DeviceBuffer<double> v;
+  detail::mixed_mult(b.m->data(), S, wB, 0, k, v);
+  std::vector<int64_t> dims;
+  Labels labels;
+  std::vector<int> lo, ro, in;
+  for (int i : o.l_outer) lo.push_back((int)dims.size()), dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  for (int j : o.r_outer) ro.push_back((int)dims.size()), dims.push_back(b.m->dim(j)), labels.push_back(b.labels[j]);
+  for (int i : o.l_inter) in.push_back((int)dims.size()), dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  SparseTensor c(dims);
+  c.take(std::move(k), std::move(v));
+  std::vector<int> rowmajor = ro;  // keys j + wB (row + h tab)
+  rowmajor.insert(rowmajor.end(), lo.begin(), lo.end());
+  rowmajor.insert(rowmajor.end(), in.begin(), in.end());
+  c.set_seq(rowmajor);
+  std::vector<int> def(dims.size());
+  std::iota(def.begin(), def.end(), 0);
+  c.change_linIdx_sequence(def);
+  c.setSorted(false);
+  return {std::move(c), std::move(labels)};
+}
+
+// DenseMIA * SparseMIA: DenseLatticeBase::operator*(SparseLatticeBase)
+// (DenseLatticeBase.h:436-500).  The sparse operand is sorted column-major
+// (under [inner, outer, inter]) and flagged unsorted; the result's keys are in
+// the default sequence, ascending, flagged sorted.
+inline SparseExpr operator*(DenseAtom a, SparseAtom b) {
+  const detail::ProductOrders o = detail::product_orders(a.labels, b.labels);
+  if (o.l_inner.empty()) throw MIAParameterException("a dense x sparse product needs a contracted index");
+  if (!detail::lattice_ordered(o.l_outer, o.l_inner, o.l_inter))
+    throw MIAParameterException("the dense operand needs its modes already in lattice order");
+  const int64_t h = detail::dense_prod(*a.m, o.l_outer), w = detail::dense_prod(*a.m, o.l_inner);
+  const int64_t d = detail::dense_prod(*a.m, o.l_inter), wB = (int64_t)detail::prod_dims(*b.m, o.r_outer);
+  if ((int64_t)detail::prod_dims(*b.m, o.r_inner) != w || (int64_t)detail::prod_dims(*b.m, o.r_inter) != d)
+    throw DimensionMismatchException("mixed product dims");
+  detail::to_lattice(*b.m, o.r_inner, o.r_outer, o.r_inter);
+  const lnt_lattice S{b.m->keys(), b.m->vals(), b.m->size(), w, wB, d};
+  DeviceBuffer<uint64_t> k;
+  DeviceBuffer<double> v;
+  detail::mixed_mult(a.m->data(), S, h, 1, k, v);
+  std::vector<int64_t> dims;
+  Labels labels;
+  for (int i : o.l_outer) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  for (int j : o.r_outer) dims.push_back(b.m->dim(j)), labels.push_back(b.labels[j]);
+  for (int i : o.l_inter) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
+  SparseTensor c(dims);
+  c.take(std::move(k), std::move(v));
+  c.setSorted(true);
+  return {std::move(c), std::move(labels)};
+}
+
 template <size_t N>
 class DenseNT : public DenseTensor {
  public:

@@ -432,6 +432,66 @@ def nolattice_mult(ak, av, h, d, bk, bv, wB):
     return np.concatenate(keys), np.concatenate(vals)
 
 
+def _lines(sk, W):
+    """Start offsets and values g = key // W of the runs of equal g in sorted keys."""
+    g = sk // np.uint64(W)
+    if g.size == 0:
+        return np.zeros(1, np.int64), g
+    heads = np.flatnonzero(np.concatenate([[True], g[1:] != g[:-1]]))
+    return np.append(heads, g.size), g[heads]
+
+
+def dense_sparse_mult(A, sk, sv, h, w, wB, d):
+    """DenseLatticeBase::operator*(SparseLatticeBase) (DenseLatticeBase.h:
+    436-500): A dense h x w x d (column-major, flat), S w x wB x d key-sorted
+    column-major.  For every (tab, col) of S with entries, in key order, h
+    outputs with keys i + h (col + wB tab): c = 0, then c = c + v * A(i, row,
+    tab) for the column's entries in order (zeros kept).  Ascending keys."""
+    A = np.asarray(A, np.float64).reshape(-1)
+    sk = np.asarray(sk, np.uint64)
+    sv = np.asarray(sv, np.float64)
+    starts, gs = _lines(sk, w)
+    keys, vals = [], []
+    for q, g in enumerate(gs):
+        t = int(g) // wB
+        c = np.zeros(h)
+        for k in range(starts[q], starts[q + 1]):
+            r = int(sk[k]) % w
+            c = c + sv[k] * A[h * (r + w * t): h * (r + w * t) + h]
+        keys.append(np.arange(h, dtype=np.uint64) + np.uint64(h) * g)
+        vals.append(c)
+    if not keys:
+        return np.zeros(0, np.uint64), np.zeros(0, np.float64)
+    return np.concatenate(keys), np.concatenate(vals)
+
+
+def sparse_dense_mult(sk, sv, B, h, w, wB, d):
+    """SparseLatticeBase::operator*(DenseLatticeBase) (SparseLatticeBase.h:
+    1148-1162), which the reference evaluates as (B^T S^T)^T through the dense
+    x sparse product: S h x w x d key-sorted ROW-major (col + w (row + h
+    tab)), B dense w x wB x d (column-major, flat).  For every (tab, row) of S
+    with entries, in key order, wB outputs with the row-major lattice keys
+    j + wB (row + h tab): c = 0, then c = c + v * B(col, j, tab) for the row's
+    entries in order.  Ascending keys."""
+    B = np.asarray(B, np.float64).reshape(-1)
+    sk = np.asarray(sk, np.uint64)
+    sv = np.asarray(sv, np.float64)
+    starts, gs = _lines(sk, w)
+    js = np.arange(wB, dtype=np.int64)
+    keys, vals = [], []
+    for q, g in enumerate(gs):
+        t = int(g) // h
+        c = np.zeros(wB)
+        for k in range(starts[q], starts[q + 1]):
+            col = int(sk[k]) % w
+            c = c + sv[k] * B[col + w * (js + wB * t)]
+        keys.append(np.arange(wB, dtype=np.uint64) + np.uint64(wB) * g)
+        vals.append(c)
+    if not keys:
+        return np.zeros(0, np.uint64), np.zeros(0, np.float64)
+    return np.concatenate(keys), np.concatenate(vals)
+
+
 def product(a: SparseMIA, a_labels, b: SparseMIA, b_labels):
     """Product a(a_labels) * b(b_labels) (MIA_Atom::operator*, MIA_Expr.h:
     864-925 with inner indices: a lattice product; 1012-1057 without: noLatticeMult).
@@ -463,6 +523,44 @@ def product(a: SparseMIA, a_labels, b: SparseMIA, b_labels):
         raise ValueError("lattice dimension mismatch")
     ck, cv = lattice_mult(ak, av, h, w, d, bk, bv, wB)
     return SparseMIA(dims, ck, cv, list(range(len(dims))), True), labels
+
+
+def mixed_product(s: SparseMIA, s_labels, D, d_dims, d_labels, dense_first: bool):
+    """MIA_Atom::operator* with one sparse and one dense operand (MIA_Expr.h:
+    864-925): the dense operand's modes are already in lattice order (zero-copy
+    DenseMIA::toStraightLattice, DenseMIA.h:1240-1255); the sparse operand is
+    sorted into its lattice and flagged unsorted.  dense_first: D * s through
+    dense_sparse_mult, result sorted in the default sequence.  Otherwise s * D
+    through sparse_dense_mult (s sorted under [inner, outer, inter], the
+    row-major lattice), result re-keyed from the row-major lattice to the
+    default sequence and flagged unsorted (SparseMIA.h:362-372).  Returns
+    (C, c_labels) with C dims [left outer, right outer, inter]."""
+    def pd(dims, modes):
+        return int(np.prod([dims[i] for i in modes], dtype=np.int64)) if modes else 1
+    if dense_first:
+        o = product_orders(d_labels, s_labels)
+        h, w, d = pd(d_dims, o["l_outer"]), pd(d_dims, o["l_inner"]), pd(d_dims, o["l_inter"])
+        wB = pd(s.dims, o["r_outer"])
+        bk, bv, _, _, _ = to_lattice(s, o["r_inner"], o["r_outer"], o["r_inter"])
+        ck, cv = dense_sparse_mult(D, bk, bv, h, w, wB, d)
+        dims = [d_dims[i] for i in o["l_outer"]] + [s.dims[j] for j in o["r_outer"]] + [d_dims[i] for i in o["l_inter"]]
+        labels = [d_labels[i] for i in o["l_outer"]] + [s_labels[j] for j in o["r_outer"]] + \
+                 [d_labels[i] for i in o["l_inter"]]
+        return SparseMIA(dims, ck, cv, list(range(len(dims))), True), labels
+    o = product_orders(s_labels, d_labels)
+    h, w, d = pd(s.dims, o["l_outer"]), pd(s.dims, o["l_inner"]), pd(s.dims, o["l_inter"])
+    wB = pd(d_dims, o["r_outer"])
+    ak, av, _, _, _ = to_lattice(s, o["l_inner"], o["l_outer"], o["l_inter"])
+    ck, cv = sparse_dense_mult(ak, av, D, h, w, wB, d)
+    dims = [s.dims[i] for i in o["l_outer"]] + [d_dims[j] for j in o["r_outer"]] + [s.dims[i] for i in o["l_inter"]]
+    labels = [s_labels[i] for i in o["l_outer"]] + [d_labels[j] for j in o["r_outer"]] + \
+             [s_labels[i] for i in o["l_inter"]]
+    nl, nr, ni = len(o["l_outer"]), len(o["r_outer"]), len(o["l_inter"])
+    rowmajor = list(range(nl, nl + nr)) + list(range(nl)) + list(range(nl + nr, nl + nr + ni))
+    c = SparseMIA(dims, ck, cv, rowmajor, True)
+    c.change_linIdx_sequence(list(range(len(dims))))
+    c.sorted = False
+    return c, labels
 
 
 def unary_orders(labels) -> dict:

@@ -7,7 +7,8 @@
 // Files: <name>.keys (uint64), <name>.vals (float64), <name>.meta (text:
 // order, dims..., seq..., sorted).  Scenarios: product, product_assign,
 // elementwise, outer_inter, outer, trace, attract, merge_add, merge_sub,
-// merge_self, plus_equals, sort_seq, collect, dense.
+// merge_self, plus_equals, sort_seq, collect, dense, mixed_sd, mixed_sd_inter,
+// mixed_ds, mixed_ds_inter.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -158,6 +159,32 @@ int main(int argc, char** argv) {
       load(a, "a");
       a.collect_duplicates();
       save(a, "c");
+    } else if (sc.rfind("mixed_", 0) == 0) {  // sparse x dense / dense x sparse
+      std::ifstream meta(g_dir + "/D.meta");
+      int64_t e0, e1, e2;
+      meta >> e0 >> e1 >> e2;
+      lnt::DenseNT<3> D(e0, e1, e2);
+      D.upload(read_raw<double>(g_dir + "/D.vals"));
+      lnt::SparseNT<3> s;
+      load(s, "a");
+      if (sc == "mixed_sd") {
+        lnt::SparseNT<2> c;
+        c(i, l) = s(i, j, k) * D(j, k, l);
+        save(c, "c");
+      } else if (sc == "mixed_sd_inter") {
+        lnt::SparseNT<3> c;
+        c(i, l, !n) = s(i, j, !n) * D(j, l, !n);
+        save(c, "c");
+      } else if (sc == "mixed_ds") {
+        lnt::SparseNT<2> c;
+        c(i, l) = D(i, j, k) * s(k, l, j);
+        save(c, "c");
+      } else {
+        lnt::SparseNT<3> c;
+        c(i, l, !n) = D(i, j, !n) * s(l, j, !n);
+        save(c, "c");
+      }
+      save(s, "a_after");
     } else if (sc == "dense") {
       std::ifstream meta(g_dir + "/dense.meta");
       int64_t d1, d2;

@@ -196,3 +196,25 @@ def test_dense_product(driver, tmp_path, rng, slices):
     got = np.frombuffer((tmp_path / "C.vals").read_bytes(), np.float64)
     ref = oracle.dense_lattice_mult(A, B, d1 * d1, d2 * d2, d1 * d1, 1)
     np.testing.assert_allclose(got, ref, rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("scenario,s_dims,s_lab,d_dims,d_lab,dense_first", [
+    ("mixed_sd", [30, 20, 10], ["i", "j", "k"], [20, 10, 40], ["j", "k", "l"], False),
+    ("mixed_sd_inter", [30, 20, 6], ["i", "j", "!n"], [20, 40, 6], ["j", "l", "!n"], False),
+    ("mixed_ds", [10, 40, 20], ["k", "l", "j"], [30, 20, 10], ["i", "j", "k"], True),
+    ("mixed_ds_inter", [40, 20, 6], ["l", "j", "!n"], [30, 20, 6], ["i", "j", "!n"], True),
+])
+def test_mixed_products(driver, tmp_path, rng, scenario, s_dims, s_lab, d_dims, d_lab, dense_first):
+    """c(i,l) = s(i,j,k) * D(j,k,l) and c(i,l) = D(i,j,k) * s(k,l,j) (with and
+    without an element-wise index): keys, sequence, sorted flag and values of
+    the result, and the sparse operand's post-state, against the oracle."""
+    s = rand_mia(rng, s_dims, 1500)
+    D = rng.uniform(-1, 1, int(np.prod(d_dims)))
+    write(tmp_path, "a", s)
+    (tmp_path / "D.vals").write_bytes(D.tobytes())
+    (tmp_path / "D.meta").write_text(" ".join(map(str, d_dims)) + "\n")
+    run(driver, scenario, tmp_path)
+    es = s.copy()
+    c, _ = oracle.mixed_product(es, s_lab, D, d_dims, d_lab, dense_first)
+    same(read(tmp_path, "c"), c, atol=0)
+    same(read(tmp_path, "a_after"), es, atol=0)

@@ -207,3 +207,24 @@ def test_sort_merge_both_paths(cuda, torch, rng, monkeypatch, path, dims, n_each
     else:  # same stable order and sequential fold: identical sums
         np.testing.assert_array_equal(to_host(v), ev)
     assert cuda.device_status() == 0
+
+
+def test_sort_reduce_clustered_buckets(cuda, torch, rng):
+    """36-bit keys, 2 x 2^20 pairs (512 buckets of about 4096): in even buckets
+    every pair shares the next 12 key bits, so one sub-bucket holds the whole
+    bucket and the local LSD passes sort it (with about 250 duplicate keys per
+    bucket); odd buckets take the counting rank.  Keys and values exact."""
+    n = 1 << 20
+    top = rng.integers(0, 1 << 9, 2 * n).astype(np.uint64)
+    mid = rng.integers(0, 1 << 12, 2 * n).astype(np.uint64)
+    mid[top % 2 == 0] = 0
+    keys = (top << np.uint64(27)) | (mid << np.uint64(15)) | rng.integers(0, 1 << 15, 2 * n).astype(np.uint64)
+    vals = rng.uniform(-1, 1, 2 * n)
+    vals[rng.random(2 * n) < 0.1] = 0.0
+    k, v = cuda.sort_reduce(to_dev(keys[:n], torch), to_dev(vals[:n], torch), to_dev(keys[n:], torch),
+                            to_dev(vals[n:], torch), max_key=1 << 36)
+    sk, sv = oracle.sort_pairs(keys, vals)
+    ek, ev = oracle.collect_duplicates(sk, sv)
+    np.testing.assert_array_equal(to_host(k, np.uint64), ek)
+    np.testing.assert_array_equal(to_host(v), ev)
+    assert cuda.device_status() == 0

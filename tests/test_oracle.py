@@ -317,3 +317,91 @@ def test_contract_attract_drops_zero_sums():
     m = oracle.SparseMIA([2, 2, 3], np.array([0, 3, 10], np.uint64), np.array([1.0, -1.0, 5.0]), sorted=False)
     c, lab = oracle.unary(m, ["i", "i", "k"])   # k = 0: (0,0,0) and (1,1,0) cancel; (0,1,2) is off the diagonal
     assert lab == ["k"] and c.keys.size == 0
+
+
+# ---- mixed sparse / dense lattice products ------------------------------------
+
+MIXED_SHAPES = [(20, 20, 20, 20), (1, 20, 1, 20), (20, 1, 20, 20), (20, 20, 20, 1), (20, 1, 1, 20)]
+
+
+def mixed_case(rng, m1, n1, n2, p):
+    """The reference's mixedlatticemulttests.cpp:13-40 set-up: dense lattices
+    with entries U[0,10), those below 7 zeroed; the sparse operands hold their
+    non-zeros."""
+    A = rng.uniform(0, 10, m1 * n1 * p)
+    B = rng.uniform(0, 10, n1 * n2 * p)
+    A[A < 7] = 0.0
+    B[B < 7] = 0.0
+    return A, B
+
+
+def dense_tabs(A, B, m1, n1, n2, p):
+    """(p, m1, n2) per-tab products of column-major flat lattices."""
+    return np.stack([A.reshape(p, n1, m1)[t].T @ B.reshape(p, n2, n1)[t].T for t in range(p)])
+
+
+def rowmajor_keys(flat_colmajor_idx, rows, cols):
+    r, c, t = flat_colmajor_idx % rows, (flat_colmajor_idx // rows) % cols, flat_colmajor_idx // (rows * cols)
+    return c + cols * (r + rows * t)
+
+
+@pytest.mark.parametrize("m1,n1,n2,p", MIXED_SHAPES)
+def test_mixed_products_match_dense(rng, m1, n1, n2, p):
+    """mixedlatticemulttests.cpp: sparse x dense and dense x sparse equal the
+    dense product (fuzzy); every non-empty line of the sparse operand gives a
+    full line of the result, other entries are absent."""
+    A, B = mixed_case(rng, m1, n1, n2, p)
+    Cd = dense_tabs(A, B, m1, n1, n2, p)
+    # dense x sparse: B sparse, column-major keys
+    bk = np.flatnonzero(B).astype(np.uint64)
+    k, v = oracle.dense_sparse_mult(A, bk, B[bk.astype(np.int64)], m1, n1, n2, p)
+    assert np.all(k[1:] > k[:-1])
+    expect_cols = np.unique(bk // np.uint64(n1))
+    assert k.size == expect_cols.size * m1
+    flat = np.transpose(Cd, (0, 2, 1)).reshape(-1)
+    np.testing.assert_allclose(v, flat[k.astype(np.int64)], rtol=1e-12, atol=1e-9)
+    # sparse x dense: A sparse, row-major keys (col + n1 (row + m1 tab))
+    nz = np.flatnonzero(A)
+    rk = rowmajor_keys(nz, m1, n1)
+    order = np.argsort(rk, kind="stable")
+    k2, v2 = oracle.sparse_dense_mult(rk[order].astype(np.uint64), A[nz][order], B, m1, n1, n2, p)
+    assert np.all(k2[1:] > k2[:-1])
+    assert k2.size == np.unique(rk // n1).size * n2
+    np.testing.assert_allclose(v2, Cd.reshape(-1)[k2.astype(np.int64)], rtol=1e-12, atol=1e-9)
+
+
+def test_mixed_products_keep_zero_lines():
+    """A line of the sparse operand whose products cancel still gives a full
+    line of exact zeros (the reference writes every entry of the line)."""
+    A = np.array([1.0, 2.0, 1.0, 2.0])              # 2 x 2 x 1: A(:,0) = A(:,1) = (1, 2)
+    bk = np.array([0, 1], np.uint64)                # S(0,0) = 3, S(1,0) = -3 (2 x 1 x 1)
+    k, v = oracle.dense_sparse_mult(A, bk, np.array([3.0, -3.0]), 2, 2, 1, 1)
+    np.testing.assert_array_equal(k, np.array([0, 1], np.uint64))
+    np.testing.assert_array_equal(v, np.array([0.0, 0.0]))
+
+
+@pytest.mark.parametrize("s_dims,s_lab,d_dims,d_lab,dense_first,sub", [
+    ([6, 5, 4], ["i", "j", "k"], [5, 4, 7], ["j", "k", "l"], False, "ijk,jkl->il"),
+    ([6, 5, 3], ["i", "j", "!n"], [5, 7, 3], ["j", "l", "!n"], False, "ijn,jln->iln"),
+    ([4, 7, 5], ["k", "l", "j"], [6, 5, 4], ["i", "j", "k"], True, "ijk,klj->il"),
+    ([7, 5, 3], ["l", "j", "!n"], [6, 5, 3], ["i", "j", "!n"], True, "ijn,ljn->iln"),
+])
+def test_mixed_product_vs_dense(rng, s_dims, s_lab, d_dims, d_lab, dense_first, sub):
+    """MIA-level mixed products against einsum: values of the kept lines, every
+    other entry of the dense result zero; the sorted flag per side."""
+    total = int(np.prod(s_dims))
+    keys = rng.choice(total, 40, replace=False).astype(np.uint64)
+    s = oracle.SparseMIA(s_dims, keys, rng.uniform(-1, 1, 40), sorted=False)
+    D = rng.uniform(-1, 1, int(np.prod(d_dims)))
+    Sd = np.zeros(total)
+    Sd[keys.astype(np.int64)] = s.vals
+    Sd = Sd.reshape(s_dims[::-1]).transpose()          # column-major: first mode fastest
+    Dd = D.reshape(d_dims[::-1]).transpose()
+    Cd = np.einsum(sub, Dd, Sd) if dense_first else np.einsum(sub, Sd, Dd)
+    c, labels = oracle.mixed_product(s.copy(), s_lab, D, d_dims, d_lab, dense_first)
+    assert c.seq == list(range(c.order)) and c.sorted == dense_first
+    flat = Cd.transpose().reshape(-1)
+    np.testing.assert_allclose(c.vals, flat[c.keys.astype(np.int64)], rtol=1e-12, atol=1e-12)
+    rest = np.ones(flat.size, bool)
+    rest[c.keys.astype(np.int64)] = False
+    assert np.all(flat[rest] == 0.0)
