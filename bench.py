@@ -896,6 +896,105 @@ def run_outer(args):
     return 0
 
 
+def run_mixed(args):
+    """Mixed lattice products: c(i,l) = A(i,j) * s(j,l) with A dense 2048 x 8192
+    (128 MB, about the L2) and s sparse 8192 x 16384 with 2^21 distinct uniform
+    entries (128 per column), key-sorted column-major; a step = count +
+    product through the C ABI (dense x sparse).  The sparse x dense product
+    s'(l,j) * A'(j,i) on the transposed data (its transpose of the dense operand
+    included) is timed the same way and reported in config.  Each (entry, row)
+    is one multiply and one add on an element of A gathered from L2."""
+    import ctypes as C
+
+    import torch
+
+    import libnt_b200 as L
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    h, w, wB = 2048, 8192, 16384 >> args.shrink
+    nnz = 1 << (21 - args.shrink)
+    A = torch.rand(h * w, generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    sk = torch.unique(torch.randint(0, w * wB, (nnz,), generator=g, device=dev))
+    sv = torch.rand(sk.numel(), generator=g, device=dev, dtype=torch.float64) * 2 - 1
+    lib = L.lib()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def setup(D, S, other, dense_first):
+        nb_ = C.c_size_t(0)
+        L._check(lib.lnt_sparse_dense_mult_workspace(C.byref(S), other, dense_first, C.byref(nb_)), "workspace")
+        ws = L.workspace(nb_.value, dev)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        L._check(lib.lnt_sparse_dense_mult_count(C.byref(S), other, dense_first, C.c_void_p(ws.data_ptr()),
+                                                 ws.numel(), C.c_void_p(cnt.data_ptr()), stream), "count")
+        n_out = int(cnt.item())
+        ck = torch.empty(n_out, dtype=torch.int64, device=dev)
+        cv = torch.empty(n_out, dtype=torch.float64, device=dev)
+
+        def step():
+            L._check(lib.lnt_sparse_dense_mult_count(C.byref(S), other, dense_first, C.c_void_p(ws.data_ptr()),
+                                                     ws.numel(), C.c_void_p(cnt.data_ptr()), stream), "count")
+            L._check(lib.lnt_sparse_dense_mult(C.c_void_p(D.data_ptr()), C.byref(S), other, dense_first,
+                                               C.c_void_p(ws.data_ptr()), ws.numel(), C.c_void_p(ck.data_ptr()),
+                                               C.c_void_p(cv.data_ptr()), stream), "mult")
+        return step, n_out, ck, cv
+
+    S = L.Lattice.of(sk, sv, w, wB, 1)
+    step, n_out, ck, cv = setup(A, S, h, 1)
+    ms, launches, clocks = _timed_steps(torch, step, args)
+    prod_ms = L.profile_query("mixed_product")[0] / args.steps
+    ms = max_over_ranks(ms, world)
+    # spot check: the first output against a float64 recomputation from the inputs
+    col = int(ck[0].item()) // h
+    rows = sk[(sk // w) == col] % w
+    vals = sv[(sk // w) == col]
+    acc = torch.zeros((), dtype=torch.float64, device=dev)
+    for r, v in zip(rows.tolist(), vals.tolist()):
+        acc = acc + v * A[int(r) * h]
+    assert L.device_status() == 0 and n_out == int(torch.unique(sk // w).numel()) * h
+    assert float(acc.item()) == float(cv[0].item())
+    # sparse x dense on the transposed operands, c'(l,i) = s'(l,j) * B(j,i) with s' = s^T (its row-major
+    # keys j + w l are s's column-major keys) and B = A^T (w x h, column-major)
+    S2 = L.Lattice.of(sk, sv, wB, w, 1)
+    step2, _, _, _ = setup(A.view(w, h).t().contiguous().view(-1), S2, h, 0)
+    ms2, _, _ = _timed_steps(torch, step2, args)
+    sd_kernels = {k: L.profile_query(k)[0] / args.steps for k in ("mixed_count", "mixed_transpose", "mixed_product")}
+    if rank != 0:
+        return 0
+    peak, peak_kind = peaks()
+    flops = 2.0 * sk.numel() * h
+    alg = 8.0 * h * w + 16.0 * sk.numel() + 16.0 * n_out
+    gathered = 8.0 * sk.numel() * h
+    cpu = None
+    if not args.no_cpu and world == 1:
+        import oracle
+        rng = np.random.default_rng(1)
+        cw, cwB = 8192, 64
+        cA = rng.uniform(-1, 1, h * cw)
+        csk = np.unique(rng.integers(0, cw * cwB, 1 << 13, dtype=np.uint64))
+        t0 = time.perf_counter()
+        oracle.dense_sparse_mult(cA, csk, rng.uniform(-1, 1, csk.size), h, cw, cwB, 1)
+        t = time.perf_counter() - t0
+        cpu = {"value": 2.0 * csk.size * h / t / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
+               "sample": f"A 2048 x 8192, s 8192 x 64 with {csk.size} entries: the restated dense x sparse loop "
+                         "(numpy, one column of A per entry), one thread"}
+    config = {"workload": "dense x sparse c(i,l) = A(i,j) * s(j,l): A 2048 x 8192 dense, s 8192 x 16384 with "
+                          "2^21 uniform distinct entries; step = count + product",
+              "nnz": int(sk.numel()), "outputs": n_out, "product_ms": prod_ms,
+              "l2_gather_GBs": gathered / (prod_ms * 1e-3) / 1e9,
+              "sparse_x_dense_ms_per_step": ms2, "sparse_x_dense_kernels_ms": sd_kernels,
+              "l2": "A (128 MB) about the L2; the output (537 MB) far larger", "parallelism": "1 GPU"}
+    print(json.dumps(_line("GFLOP/s", flops * world / (ms * 1e-3) / 1e9, ms, args, world, config, {
+        "gpu_launches": launches, "cpu_baseline": cpu, "clocks": clocks,
+        "roofline": {"bound": "hbm", "kernel": "mixed_product", "achieved": alg / (prod_ms * 1e-3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": alg / (prod_ms * 1e-3) / 1e9 / peak,
+                     "alg_bytes_per_launch": alg, "avg_launch_ms": prod_ms, "peak_source": peak_kind,
+                     "traffic": None},
+    })), flush=True)
+    return 0
+
+
 def run_unary(args):
     """Unary contraction (contract_attract): b(k) = a(i,i,k), a 8192 x 8192 x 1024
     with 2^26 entries (uniform, distinct, key-sorted under [i, i, k]); a step =
@@ -1211,7 +1310,7 @@ def main():
     ap.add_argument("--nnz-log2", type=int, default=26,
                     help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
-    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed", "outer", "unary", "scanmerge"],
+    ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed", "outer", "unary", "scanmerge", "mixed"],
                     help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
                          "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")
     ap.add_argument("--slices", type=int, default=7, help="dense scheme I: INT8 slices per operand")
@@ -1235,7 +1334,7 @@ def main():
         return run_reference(args)
     return {"merge": run_ours, "contraction": run_contraction, "batched": run_batched,
             "dense": run_dense, "skewed": run_skewed, "outer": run_outer, "unary": run_unary,
-            "scanmerge": run_scanmerge}[args.workload](args)
+            "scanmerge": run_scanmerge, "mixed": run_mixed}[args.workload](args)
 
 
 if __name__ == "__main__":
