@@ -60,7 +60,19 @@ class RekeySpec(C.Structure):
 
 _vp = C.c_void_p
 _sz = C.c_size_t
+# lnt_host_alloc (include/lnt_mex.h): void* (*)(size_t); HostAlloc() is the NULL
+# pointer (the gateway then uses malloc)
+HostAlloc = C.CFUNCTYPE(C.c_void_p, C.c_size_t)
+_pvp = C.POINTER(C.c_void_p)
+_psz = C.POINTER(C.c_size_t)
+_MEX_OUT = [HostAlloc, _pvp, _pvp, _psz]
 _SIGS = {
+    "lnt_mex_sparse_sort": ([_vp, _vp, _sz], C.c_int),
+    "lnt_mex_sparse_change_linidx": ([_vp, _sz, C.c_int, _vp, _vp, _vp], C.c_int),
+    "lnt_mex_sparse_permute": ([_vp, _vp, _sz, C.c_int, _vp, _vp, _vp], C.c_int),
+    "lnt_mex_sparse_merge": ([_vp, _vp, _sz, _vp, _vp, _sz, C.c_int] + _MEX_OUT, C.c_int),
+    "lnt_mex_sparselattice_mult": ([_vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, C.c_int] + _MEX_OUT, C.c_int),
+    "lnt_mex_sparse_denselattice_mult": ([_vp, _vp, _sz, _vp, _vp, _vp, C.c_int] + _MEX_OUT, C.c_int),
     "lnt_status_string": ([C.c_int], C.c_char_p),
     "lnt_version": ([], C.c_int),
     "lnt_launch_count": ([], C.c_uint64),

@@ -1,9 +1,10 @@
 """CPU checks of the C ABI: the library loads, exports every function that
-include/lnt.h declares, and rejects bad arguments before touching a GPU."""
+include/*.h declare, and rejects bad arguments before touching a GPU."""
 import ctypes as C
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 import libnt_b200 as L
@@ -12,7 +13,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 
 def header_symbols():
-    text = (ROOT / "include" / "lnt.h").read_text()
+    text = "".join(h.read_text() for h in sorted((ROOT / "include").glob("*.h")))
     return sorted(set(re.findall(r"LNT_API\s+[\w\s\*]+?\b(lnt_\w+)\s*\(", text)))
 
 
@@ -24,7 +25,7 @@ def test_header_declares_entry_points():
 def test_library_exports_every_declared_symbol():
     lib = L.lib()
     for s in header_symbols():
-        assert hasattr(lib, s), f"{s} declared in include/lnt.h but not exported"
+        assert hasattr(lib, s), f"{s} declared in include/*.h but not exported"
 
 
 def test_python_bindings_cover_header():
@@ -68,3 +69,34 @@ def test_sort_rejects_small_workspace_without_gpu():
     lib = L.lib()
     d = C.c_void_p(256)
     assert lib.lnt_sort_pairs(d, d, d, d, 1000, 1 << 20, d, 16, None) == 5  # LNT_WORKSPACE
+
+
+def test_mex_gateways_reject_bad_arguments_without_gpu():
+    """The mex-format host gateways (include/lnt_mex.h) check their arguments
+    before any device work: 1-based orders, non-negative keys, the lattice
+    product algorithm and shapes."""
+    lib = L.lib()
+    keys = np.array([3, 1, 2], np.int64)
+    vals = np.ones(3)
+    dims = np.array([4, 5], np.int64)
+    bad = np.array([1, 1], np.uint8)    # not a permutation
+    zero = np.array([0, 1], np.uint8)   # 0 is not a 1-based index
+    ok = np.array([1, 2], np.uint8)
+    assert lib.lnt_mex_sparse_change_linidx(keys.ctypes.data, 3, 2, bad.ctypes.data, ok.ctypes.data,
+                                            dims.ctypes.data) == 3
+    assert lib.lnt_mex_sparse_permute(vals.ctypes.data, keys.ctypes.data, 3, 2, ok.ctypes.data, zero.ctypes.data,
+                                      dims.ctypes.data) == 3
+    neg = np.array([3, -1, 2], np.int64)
+    assert lib.lnt_mex_sparse_sort(vals.ctypes.data, neg.ctypes.data, 3) == 1
+    cv, ck, nc = C.c_void_p(), C.c_void_p(), C.c_size_t()
+    d3 = np.array([4, 5, 1], np.int64)
+    e3 = np.array([6, 2, 1], np.int64)   # rows(B) != cols(A)
+    args = (vals.ctypes.data, keys.ctypes.data, 3, d3.ctypes.data, vals.ctypes.data, keys.ctypes.data, 3)
+    assert lib.lnt_mex_sparselattice_mult(*args, d3.ctypes.data, 1, L.HostAlloc(), C.byref(cv), C.byref(ck),
+                                          C.byref(nc)) == 8   # csc_times: not this product
+    assert lib.lnt_mex_sparselattice_mult(*args, e3.ctypes.data, 0, L.HostAlloc(), C.byref(cv), C.byref(ck),
+                                          C.byref(nc)) == 2
+    B = np.ones(12)
+    assert lib.lnt_mex_sparse_denselattice_mult(vals.ctypes.data, keys.ctypes.data, 3, d3.ctypes.data,
+                                                B.ctypes.data, e3.ctypes.data, 0, L.HostAlloc(), C.byref(cv), C.byref(ck),
+                                                C.byref(nc)) == 2
