@@ -16,12 +16,13 @@
 //                   tab(g) = g / h; the keys are the reference's row-major
 //                   lattice keys j + wB (row + h tab).
 // Pipeline: count (segment heads -> scan -> segment table), [transpose],
-// product.  Product: one CTA per (segment, chunk of 1024 outputs), 256
-// threads x 4 outputs; the segment's entries are staged in shared memory 256
-// at a time and every output accumulates acc = acc + v * m with a separate
-// multiply and add (the reference's c += b * a, not contracted) in key order,
-// so results are bit-exact.  HBM-bound: 8 B of M per (entry, output) from L2
-// or DRAM, 16 B written per output.
+// product.  Product: one CTA job per (chunk of 512 output rows, segment),
+// chunk-major, 256 threads x 2 outputs; the segment's entries are staged in
+// shared memory 256 at a time and every output accumulates acc = acc + v * m
+// with a separate multiply and add (the reference's c += b * a, not
+// contracted) in key order, so results are bit-exact.  Bound by the gather of
+// M: 8 B of M per (entry, output) from L2 (chunk-major jobs keep 512 rows of M
+// resident), 16 B written per output.
 #include <algorithm>
 
 #include "lnt_scan.cuh"
@@ -30,7 +31,7 @@ namespace lnt {
 namespace {
 
 constexpr int kMT = 256;            // product CTA threads
-constexpr int kMQ = 4;              // outputs per thread
+constexpr int kMQ = 2;              // outputs per thread
 constexpr int kMChunk = kMT * kMQ;  // outputs per CTA job
 constexpr int kTT = 32;             // transpose tile
 
@@ -90,10 +91,14 @@ __global__ void __launch_bounds__(kMT) mixed_product_kernel(const u64* __restric
   __shared__ u64 s_inner[kMT];
   __shared__ double s_v[kMT];
   const int tid = threadIdx.x;
-  const u64 jobs = *d_nseg * chunks;
+  // chunk-major: the CTAs in flight share one chunk of the output rows, so the
+  // dense operand's working set is kMChunk rows of it, which stays in L2
+  const u64 nseg = *d_nseg;
+  const u64 jobs = nseg * chunks;
   for (u64 job = blockIdx.x; job < jobs; job += gridDim.x) {
-    const u64 s = job / chunks;
-    const u64 q0 = (job - s * chunks) * kMChunk;
+    const u64 chunk = job / nseg;
+    const u64 s = job - chunk * nseg;
+    const u64 q0 = chunk * kMChunk;
     const u64 g = seg_g[s], t = divide(g, td);
     const u64 lo = seg_start[s], hi = t < tabs ? seg_start[s + 1] : lo;  // keys past the last tab add nothing
     const double* Mt = M + Q * wd.d * (t < tabs ? t : 0);
