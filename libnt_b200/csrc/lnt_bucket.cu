@@ -165,6 +165,11 @@ __device__ __forceinline__ u32 match7(u32 d) {
   return peers;
 }
 
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
 // Shared-memory slot of bucket position p: one spare word per 32 keeps
 // blocked (stride-kBItems) accesses free of bank conflicts.
 __device__ __forceinline__ u32 slot(u32 p) { return p + (p >> 5); }
@@ -202,16 +207,19 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
   const u64 lowmask = (1ull << low_bits) - 1ull;
   const u32 warp_base = warp * kBItems * 32;
 
-  // ---- load: packed (low key << 13 | local index), values to shared memory ----
+  // ---- load: packed (low key << 13 | local index); the values go to shared
+  // memory by asynchronous copies that complete while the keys are sorted ----
+#pragma unroll
+  for (int i = 0; i < kBItems; ++i) {
+    const u32 p = warp_base + i * 32 + lane;
+    if (p < cnt) cp_async8(&s_v[slot(p)], vals + start + p);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
   u64 w[kBItems];
 #pragma unroll
   for (int i = 0; i < kBItems; ++i) {
     const u32 p = warp_base + i * 32 + lane;
-    w[i] = 0;
-    if (p < cnt) {
-      w[i] = ((__ldcs(keys + start + p) & lowmask) << kIdxBits) | p;
-      s_v[slot(p)] = __ldcs(vals + start + p);
-    }
+    w[i] = p < cnt ? ((__ldcs(keys + start + p) & lowmask) << kIdxBits) | p : 0ull;
   }
 
   // ---- counting pass over the top sub-bucket bits ----------------------------
@@ -368,6 +376,8 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
     }
   }
   }  // clustered keys
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();  // every thread's value copies have landed
 
   // ---- fold runs of equal keys (they all lie in this bucket) ------------------
   const u64 prefix = (u64)b << low_bits;
