@@ -409,7 +409,11 @@ __global__ void __launch_bounds__(256) residue_a_kernel(const double* __restrict
     for (int c = 0; c < 4; ++c) x[c] = rint(scale2(tile[rr][4 * lane + c], sc));
     u32* dst = reinterpret_cast<u32*>(res + i * Kp + k);
     const u64 plane = Mp * Kp / 4;
-    for (int l = 0; l < P.n; ++l) dst[(u64)l * plane] = pack_res4(x, l, P);
+#pragma unroll
+    for (int l = 0; l < kMaxModuli; ++l) {  // compile-time l: the moduli tables are direct constant operands
+      if (l >= P.n) break;
+      dst[(u64)l * plane] = pack_res4(x, l, P);
+    }
   }
 }
 
@@ -427,7 +431,11 @@ __global__ void residue_b_kernel(const double* __restrict__ B, u64 w, u64 wB, u6
       double x[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) x[c] = 4 * g + c < w ? rint(scale2(col[4 * g + c], sc)) : 0.0;
-      for (int l = 0; l < P.n; ++l) dst[(u64)l * plane + g] = pack_res4(x, l, P);
+#pragma unroll
+      for (int l = 0; l < kMaxModuli; ++l) {
+        if (l >= P.n) break;
+        dst[(u64)l * plane + g] = pack_res4(x, l, P);
+      }
     }
   }
 }
