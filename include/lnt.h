@@ -272,8 +272,9 @@ LNT_API int lnt_nolattice_mult(const lnt_lattice* A, const lnt_lattice* B, uint6
  *     tabs(S) with the reference's row-major lattice keys
  *     j + other (row + rows tab), ascending.
  * Two phases sharing one workspace: lnt_sparse_dense_mult_count finds the
- * lines of S and writes the output count to *d_count; lnt_sparse_dense_mult
- * writes C.  Keys must lie below rows * cols * tabs (entries past the last
+ * lines of S (kept in the workspace) and writes the output count to
+ * *d_count; lnt_sparse_dense_mult, called after it with the same S and
+ * workspace on the same stream, writes C.  Keys must lie below rows * cols * tabs (entries past the last
  * tab contribute nothing).  LNT_BAD_DIMS for non-positive extents. */
 LNT_API int lnt_sparse_dense_mult_workspace(const lnt_lattice* S, int64_t other, int dense_first, size_t* bytes);
 LNT_API int lnt_sparse_dense_mult_count(const lnt_lattice* S, int64_t other, int dense_first, void* workspace,
