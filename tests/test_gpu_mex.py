@@ -126,3 +126,32 @@ def test_mex_sparse_denselattice_mult(lib, rng, dense_first):
                     int(dense_first))
     np.testing.assert_array_equal(k, ek)
     np.testing.assert_array_equal(v, ev)
+
+
+def test_mex_empty_operands(lib, rng):
+    """Empty operands: sort / change_linidx / permute are no-ops; merges and
+    products return what the non-empty side gives (or nothing)."""
+    e64, ef = np.zeros(0, np.int64), np.zeros(0)
+    dims = np.array([4, 5], np.int64)
+    o12, o21 = np.array([1, 2], np.uint8), np.array([2, 1], np.uint8)
+    assert lib.lnt_mex_sparse_sort(ptr(ef), ptr(e64), 0) == 0
+    assert lib.lnt_mex_sparse_change_linidx(ptr(e64), 0, 2, ptr(o12), ptr(o21), ptr(dims)) == 0
+    assert lib.lnt_mex_sparse_permute(ptr(ef), ptr(e64), 0, 2, ptr(o12), ptr(o21), ptr(dims)) == 0
+    bk = np.array([2, 5, 9], np.int64)
+    bv = np.array([1.0, -2.0, 3.0])
+    for op in (0, 1):
+        k, v = call_out(lib.lnt_mex_sparse_merge, ptr(ef), ptr(e64), 0, ptr(bv), ptr(bk), 3, op)
+        ek, ev = oracle.merge_sorted(e64.astype(np.uint64), ef, bk.astype(np.uint64), bv, op)
+        np.testing.assert_array_equal(k, ek)
+        np.testing.assert_array_equal(v, ev)
+    k, v = call_out(lib.lnt_mex_sparse_merge, ptr(ef), ptr(e64), 0, ptr(ef), ptr(e64), 0, 0)
+    assert k.size == 0
+    d3 = np.array([3, 4, 2], np.int64)
+    e3 = np.array([4, 5, 2], np.int64)
+    k, v = call_out(lib.lnt_mex_sparselattice_mult, ptr(ef), ptr(e64), 0, ptr(d3), ptr(bv), ptr(bk), 3, ptr(e3), 0)
+    assert k.size == 0
+    B = rng.uniform(-1, 1, 4 * 5 * 2)
+    for dense_first, sd, dd in ((0, d3, e3), (1, np.array([5, 6, 2], np.int64), np.array([3, 5, 2], np.int64))):
+        k, v = call_out(lib.lnt_mex_sparse_denselattice_mult, ptr(ef), ptr(e64), 0, ptr(sd), ptr(B), ptr(dd),
+                        dense_first)
+        assert k.size == 0
