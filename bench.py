@@ -234,6 +234,9 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+E2E_LANES = 3  # copy/merge streams of the end-to-end measurement
+
+
 def run_ours(args):
     import torch
 
@@ -302,9 +305,10 @@ def run_ours(args):
 
     # ---- end-to-end through the C ABI from pinned host buffers ------------
     # Every step copies its operands host->device, merges, and copies its
-    # result (full capacity; the count comes back with it) device->host.  Two
-    # streams with their own device buffers let step i+1's host->device copy
-    # overlap step i's merge and device->host copy (PCIe is full duplex).
+    # result (full capacity; the count comes back with it) device->host.
+    # Three streams with their own buffers: a stream's next upload waits behind
+    # its own download, so with three the uploads of steps i+1 and i+2 queue
+    # back to back while step i merges and downloads (PCIe is full duplex).
     hin = [t.cpu().pin_memory() for t in (ak, av, bk, bv)]
     need = L.sort_reduce_workspace(na, nb, MAX_KEY)
 
@@ -320,10 +324,10 @@ def run_ours(args):
             self.hov = torch.empty(n, dtype=torch.float64, pin_memory=True)
             self.hcnt = torch.zeros(1, dtype=torch.int64, pin_memory=True)
 
-    lanes = [Lane(), Lane()]
+    lanes = [Lane() for _ in range(E2E_LANES)]
 
     def e2e_step(i):
-        ln = lanes[i % 2]
+        ln = lanes[i % len(lanes)]
         with torch.cuda.stream(ln.stream):
             for d, h in zip(ln.din, hin):
                 d.copy_(h, non_blocking=True)
@@ -333,8 +337,8 @@ def run_ours(args):
             ln.hok.copy_(ln.ok, non_blocking=True)
             ln.hov.copy_(ln.ov, non_blocking=True)
 
-    e2e_steps = max(4, min(args.steps, 10))
-    for i in range(2):
+    e2e_steps = max(6, min(args.steps, 12))
+    for i in range(len(lanes)):
         e2e_step(i)
     torch.cuda.synchronize()
     barrier(world)
@@ -387,7 +391,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "nnz/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(16 * n + 8),
-                    "pipelining": "2 streams: step i+1's H2D overlaps step i's merge and D2H"},
+                    "pipelining": f"{E2E_LANES} streams: the H2D of steps i+1, i+2 overlap step i's merge and D2H"},
             "gpu_launches": launches,
             "step_alg_bytes": step_alg, "step_hbm_frac_alg": step_alg / (ms * 1e-3) / 1e9 / peak,
             "kernels": kernels,
