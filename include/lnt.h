@@ -332,6 +332,17 @@ LNT_API int lnt_batched_lattice_mult(int count, const int64_t* dims_host, const 
 
 /* ---- dense lattice product ---------------------------------------------- */
 
+/* Dense mode permutation, float64 column-major: out has extent dims[perm[k]]
+ * in mode k and out(i_0, ..., i_{order-1}) = in(j) with j_{perm[k]} = i_k.
+ * The copy that puts a dense operand's modes in lattice order before a
+ * product: latticeCopy (FunctionUtil.h:195) and DenseMIA::inplace_permute
+ * (DenseMIA.h:700-780, same reshuffle_order convention; here out of place).
+ * out must not overlap in.  LNT_BAD_SEQ when perm is not a permutation of
+ * 0..order-1. */
+LNT_API int lnt_dense_permute(const double* in, double* out, int order, const int64_t* dims,
+                              const int32_t* perm, void* stream);
+
+
 /* C(:,:,t) = A(:,:,t) * B(:,:,t) for t < d; A is h x w, B is w x wB, C is
  * h x wB, all float64 column-major, tabs stored one after another.  Replaces
  * DenseLatticeBase::operator* (DenseLatticeBase.h:404-430, an Eigen GEMM per

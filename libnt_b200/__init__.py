@@ -107,6 +107,7 @@ _SIGS = {
     "lnt_nolattice_mult_workspace": ([C.POINTER(Lattice), C.POINTER(Lattice), C.POINTER(C.c_size_t)], C.c_int),
     "lnt_nolattice_mult_count": ([C.POINTER(Lattice), C.POINTER(Lattice), _vp, _sz, _vp, _vp], C.c_int),
     "lnt_nolattice_mult": ([C.POINTER(Lattice), C.POINTER(Lattice), C.c_uint64, _vp, _sz, _vp, _vp, _vp], C.c_int),
+    "lnt_dense_permute": ([_vp, _vp, C.c_int, _vp, _vp, _vp], C.c_int),
     "lnt_sparse_dense_mult_workspace": ([C.POINTER(Lattice), C.c_int64, C.c_int, C.POINTER(C.c_size_t)], C.c_int),
     "lnt_sparse_dense_mult_count": ([C.POINTER(Lattice), C.c_int64, C.c_int, _vp, _sz, _vp, _vp], C.c_int),
     "lnt_sparse_dense_mult": ([_vp, C.POINTER(Lattice), C.c_int64, C.c_int, _vp, _sz, _vp, _vp, _vp], C.c_int),
@@ -518,6 +519,19 @@ def dense_crt_workspace(h: int, w: int, wB: int, moduli: int = 13) -> int:
     b = C.c_size_t(0)
     _check(lib().lnt_dense_crt_workspace(h, w, wB, moduli, C.byref(b)), "lnt_dense_crt_workspace")
     return b.value
+
+
+def dense_permute(x, dims, perm):
+    """Dense mode permutation (column-major): mode k of the result is mode
+    perm[k] of x.  Returns a new float64 device tensor."""
+    torch = _torch()
+    _dev(x)
+    d = np.ascontiguousarray(dims, np.int64)
+    pm = np.ascontiguousarray(perm, np.int32)
+    out = torch.empty_like(x)
+    _check(lib().lnt_dense_permute(_ptr(x), _ptr(out), len(d), d.ctypes.data, pm.ctypes.data, _stream()),
+           "lnt_dense_permute")
+    return out
 
 
 def dense_mult_crt(A, B, h: int, w: int, wB: int, d: int = 1, moduli: int = 13, out=None, ws=None):

@@ -773,20 +773,36 @@ struct DenseAtom {
   }
 };
 
+namespace detail {
+
+// A dense operand's data in the lattice order [x, y, z] (mode indices): its own
+// buffer when the modes are already in that order (toStraightLattice,
+// DenseMIA.h:1240-1255), else a permuted copy held in `copy` (latticeCopy,
+// FunctionUtil.h:195; the operand itself is left as it is).
+inline const double* lattice_data(const DenseTensor& t, const std::vector<int>& x, const std::vector<int>& y,
+                                  const std::vector<int>& z, DenseTensor& copy) {
+  std::vector<int> s = x;
+  s.insert(s.end(), y.begin(), y.end());
+  s.insert(s.end(), z.begin(), z.end());
+  bool ordered = true;
+  for (size_t i = 0; i < s.size(); ++i) ordered = ordered && s[i] == (int)i;
+  if (ordered) return t.data();
+  std::vector<int64_t> nd;
+  for (int m : s) nd.push_back(t.dim(m));
+  copy = DenseTensor(nd);
+  const std::vector<int32_t> perm(s.begin(), s.end());
+  check(lnt_dense_permute(t.data(), copy.data(), (int)t.order(), t.dims().data(), perm.data(), nullptr),
+        "dense permute");
+  return copy.data();
+}
+
+}  // namespace detail
+
 inline DenseExpr operator*(DenseAtom a, DenseAtom b) {
   const detail::ProductOrders o = detail::product_orders(a.labels, b.labels);
-  auto consecutive = [](const std::vector<int>& x, const std::vector<int>& y, const std::vector<int>& z) {
-    std::vector<int> s = x;
-    s.insert(s.end(), y.begin(), y.end());
-    s.insert(s.end(), z.begin(), z.end());
-    for (size_t i = 0; i < s.size(); ++i)
-      if (s[i] != (int)i) return false;
-    return true;
-  };
-  // zero-copy lattices (DenseMIA::toStraightLattice, DenseMIA.h:1240-1255); permuted
-  // copies (latticeCopy) are not on this path
-  if (!consecutive(o.l_outer, o.l_inner, o.l_inter) || !consecutive(o.r_inner, o.r_outer, o.r_inter))
-    throw MIAParameterException("dense product needs modes already in lattice order");
+  DenseTensor acopy, bcopy;
+  const double* ad = detail::lattice_data(*a.m, o.l_outer, o.l_inner, o.l_inter, acopy);
+  const double* bd = detail::lattice_data(*b.m, o.r_inner, o.r_outer, o.r_inter, bcopy);
   auto pd = [](const DenseTensor& t, const std::vector<int>& m) {
     int64_t p = 1;
     for (int i : m) p *= t.dim(i);
@@ -805,14 +821,12 @@ inline DenseExpr operator*(DenseAtom a, DenseAtom b) {
   if (s == 0) {
     size_t need = 0;
     check(lnt_dense_fp64_workspace(&need), "dense product");
-    check(lnt_dense_lattice_mult_fp64(a.m->data(), b.m->data(), c.data(), h, w, wB, d, scratch(need), need,
-                                      nullptr),
+    check(lnt_dense_lattice_mult_fp64(ad, bd, c.data(), h, w, wB, d, scratch(need), need, nullptr),
           "dense product");
   } else {
     size_t need = 0;
     check(lnt_dense_split_workspace(h, w, wB, s, &need), "dense product");
-    check(lnt_dense_lattice_mult_split(a.m->data(), b.m->data(), c.data(), h, w, wB, d, s, scratch(need), need,
-                                       nullptr),
+    check(lnt_dense_lattice_mult_split(ad, bd, c.data(), h, w, wB, d, s, scratch(need), need, nullptr),
           "dense product");
   }
   return {std::move(c), std::move(labels)};
@@ -821,21 +835,12 @@ inline DenseExpr operator*(DenseAtom a, DenseAtom b) {
 // ---- mixed sparse / dense products ---------------------------------------------
 // MIA_Atom::operator* with one sparse and one dense operand (MIA_Expr.h:
 // 864-925): the sparse operand becomes a sorted lattice, the dense one a
-// zero-copy lattice (DenseMIA::toStraightLattice, DenseMIA.h:1240-1255; modes
-// already in lattice order), and the lattice product is the mixed one
+// zero-copy lattice or a permuted copy (detail::lattice_data), and the lattice
+// product is the mixed one
 // (SparseDenseLatticeMultMex).  The result is sparse with dims [left outer,
 // right outer, inter]: every non-empty line of the sparse operand gives a full
 // line of it.
 namespace detail {
-
-inline bool lattice_ordered(const std::vector<int>& x, const std::vector<int>& y, const std::vector<int>& z) {
-  std::vector<int> s = x;
-  s.insert(s.end(), y.begin(), y.end());
-  s.insert(s.end(), z.begin(), z.end());
-  for (size_t i = 0; i < s.size(); ++i)
-    if (s[i] != (int)i) return false;
-  return true;
-}
 
 inline int64_t dense_prod(const DenseTensor& t, const std::vector<int>& m) {
   int64_t p = 1;
@@ -870,8 +875,6 @@ inline void mixed_mult(const double* D, const lnt_lattice& S, int64_t other, int
 inline SparseExpr operator*(SparseAtom a, DenseAtom b) {
   const detail::ProductOrders o = detail::product_orders(a.labels, b.labels);
   if (o.l_inner.empty()) throw MIAParameterException("a sparse x dense product needs a contracted index");
-  if (!detail::lattice_ordered(o.r_inner, o.r_outer, o.r_inter))
-    throw MIAParameterException("the dense operand needs its modes already in lattice order");
   const int64_t h = (int64_t)detail::prod_dims(*a.m, o.l_outer), w = (int64_t)detail::prod_dims(*a.m, o.l_inner);
   const int64_t d = (int64_t)detail::prod_dims(*a.m, o.l_inter), wB = detail::dense_prod(*b.m, o.r_outer);
   if (detail::dense_prod(*b.m, o.r_inner) != w || detail::dense_prod(*b.m, o.r_inter) != d)
@@ -880,7 +883,8 @@ inline SparseExpr operator*(SparseAtom a, DenseAtom b) {
   const lnt_lattice S{a.m->keys(), a.m->vals(), a.m->size(), h, w, d};
   DeviceBuffer<uint64_t> k;
   DeviceBuffer<double> v;
-  detail::mixed_mult(b.m->data(), S, wB, 0, k, v);
+  DenseTensor bcopy;
+  detail::mixed_mult(detail::lattice_data(*b.m, o.r_inner, o.r_outer, o.r_inter, bcopy), S, wB, 0, k, v);
   std::vector<int64_t> dims;
   Labels labels;
   std::vector<int> lo, ro, in;
@@ -907,8 +911,6 @@ inline SparseExpr operator*(SparseAtom a, DenseAtom b) {
 inline SparseExpr operator*(DenseAtom a, SparseAtom b) {
   const detail::ProductOrders o = detail::product_orders(a.labels, b.labels);
   if (o.l_inner.empty()) throw MIAParameterException("a dense x sparse product needs a contracted index");
-  if (!detail::lattice_ordered(o.l_outer, o.l_inner, o.l_inter))
-    throw MIAParameterException("the dense operand needs its modes already in lattice order");
   const int64_t h = detail::dense_prod(*a.m, o.l_outer), w = detail::dense_prod(*a.m, o.l_inner);
   const int64_t d = detail::dense_prod(*a.m, o.l_inter), wB = (int64_t)detail::prod_dims(*b.m, o.r_outer);
   if ((int64_t)detail::prod_dims(*b.m, o.r_inner) != w || (int64_t)detail::prod_dims(*b.m, o.r_inter) != d)
@@ -917,7 +919,8 @@ inline SparseExpr operator*(DenseAtom a, SparseAtom b) {
   const lnt_lattice S{b.m->keys(), b.m->vals(), b.m->size(), w, wB, d};
   DeviceBuffer<uint64_t> k;
   DeviceBuffer<double> v;
-  detail::mixed_mult(a.m->data(), S, h, 1, k, v);
+  DenseTensor acopy;
+  detail::mixed_mult(detail::lattice_data(*a.m, o.l_outer, o.l_inner, o.l_inter, acopy), S, h, 1, k, v);
   std::vector<int64_t> dims;
   Labels labels;
   for (int i : o.l_outer) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);

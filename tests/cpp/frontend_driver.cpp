@@ -7,8 +7,8 @@
 // Files: <name>.keys (uint64), <name>.vals (float64), <name>.meta (text:
 // order, dims..., seq..., sorted).  Scenarios: product, product_assign,
 // elementwise, outer_inter, outer, trace, attract, merge_add, merge_sub,
-// merge_self, plus_equals, sort_seq, collect, dense, mixed_sd, mixed_sd_inter,
-// mixed_ds, mixed_ds_inter.
+// merge_self, plus_equals, sort_seq, collect, dense, dense_perm, mixed_sd,
+// mixed_sd_inter, mixed_ds, mixed_ds_inter, mixed_sd_perm, mixed_ds_perm.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -159,6 +159,19 @@ int main(int argc, char** argv) {
       load(a, "a");
       a.collect_duplicates();
       save(a, "c");
+    } else if (sc == "dense_perm") {  // dense operands whose modes are not in lattice order
+      std::ifstream meta(g_dir + "/dense.meta");
+      int64_t d1, d2;
+      int slices;
+      meta >> d1 >> d2 >> slices;
+      lnt::DenseNT<4> a(d2, d1, d2, d1), b(d1, d2, d1, d2), c(d1, d1, d1, d1);
+      a.upload(read_raw<double>(g_dir + "/A.vals"));
+      b.upload(read_raw<double>(g_dir + "/B.vals"));
+      lnt::DenseTensor::slices() = slices;
+      c(i, j, m, n) = a(k, i, l, j) * b(m, k, n, l);
+      std::vector<double> h;
+      c.download(h);
+      write_raw(g_dir + "/C.vals", h);
     } else if (sc.rfind("mixed_", 0) == 0) {  // sparse x dense / dense x sparse
       std::ifstream meta(g_dir + "/D.meta");
       int64_t e0, e1, e2;
@@ -174,6 +187,14 @@ int main(int argc, char** argv) {
       } else if (sc == "mixed_sd_inter") {
         lnt::SparseNT<3> c;
         c(i, l, !n) = s(i, j, !n) * D(j, l, !n);
+        save(c, "c");
+      } else if (sc == "mixed_sd_perm") {
+        lnt::SparseNT<2> c;
+        c(i, l) = s(i, j, k) * D(l, k, j);
+        save(c, "c");
+      } else if (sc == "mixed_ds_perm") {
+        lnt::SparseNT<2> c;
+        c(i, l) = D(j, i, k) * s(k, l, j);
         save(c, "c");
       } else if (sc == "mixed_ds") {
         lnt::SparseNT<2> c;

@@ -100,3 +100,11 @@ def test_mex_gateways_reject_bad_arguments_without_gpu():
     assert lib.lnt_mex_sparse_denselattice_mult(vals.ctypes.data, keys.ctypes.data, 3, d3.ctypes.data,
                                                 B.ctypes.data, e3.ctypes.data, 0, L.HostAlloc(), C.byref(cv), C.byref(ck),
                                                 C.byref(nc)) == 2
+
+
+def test_dense_permute_checks_arguments_without_gpu():
+    lib = L.lib()
+    d = np.array([3, 4], np.int64)
+    assert lib.lnt_dense_permute(None, None, 2, d.ctypes.data, np.array([1, 1], np.int32).ctypes.data, None) == 3
+    assert lib.lnt_dense_permute(None, None, 2, np.array([3, 0], np.int64).ctypes.data,
+                                 np.array([1, 0], np.int32).ctypes.data, None) == 2

@@ -218,3 +218,49 @@ def test_mixed_products(driver, tmp_path, rng, scenario, s_dims, s_lab, d_dims, 
     c, _ = oracle.mixed_product(es, s_lab, D, d_dims, d_lab, dense_first)
     same(read(tmp_path, "c"), c, atol=0)
     same(read(tmp_path, "a_after"), es, atol=0)
+
+
+def colmajor_permute(x, dims, perm):
+    """Mode k of the result is mode perm[k] of x (column-major flat arrays)."""
+    return np.ravel(np.asarray(x).reshape(dims, order="F").transpose(perm), order="F")
+
+
+@pytest.mark.parametrize("slices", [0, 7])
+def test_dense_product_permuted_operands(driver, tmp_path, rng, slices):
+    """c(i,j,m,n) = a(k,i,l,j) * b(m,k,n,l): neither operand in lattice order,
+    so both go through a permuted copy (latticeCopy) first."""
+    d1, d2 = 6, 5
+    A = rng.uniform(-1, 1, d2 * d1 * d2 * d1)
+    B = rng.uniform(-1, 1, d1 * d2 * d1 * d2)
+    (tmp_path / "A.vals").write_bytes(A.tobytes())
+    (tmp_path / "B.vals").write_bytes(B.tobytes())
+    (tmp_path / "dense.meta").write_text(f"{d1} {d2} {slices}\n")
+    run(driver, "dense_perm", tmp_path)
+    got = np.frombuffer((tmp_path / "C.vals").read_bytes(), np.float64)
+    An = A.reshape([d2, d1, d2, d1], order="F")
+    Bn = B.reshape([d1, d2, d1, d2], order="F")
+    ref = np.ravel(np.einsum("kilj,mknl->ijmn", An, Bn), order="F")
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("scenario,s_dims,s_lab,d_dims,perm,d_lab,dense_first", [
+    # c(i,l) = s(i,j,k) * D(l,k,j): D's lattice order is (j, k, l) = modes [2, 1, 0]
+    ("mixed_sd_perm", [30, 20, 10], ["i", "j", "k"], [40, 10, 20], [2, 1, 0], ["j", "k", "l"], False),
+    # c(i,l) = D(j,i,k) * s(k,l,j): D's lattice order is (i, j, k) = modes [1, 0, 2]
+    ("mixed_ds_perm", [10, 40, 20], ["k", "l", "j"], [20, 30, 10], [1, 0, 2], ["i", "j", "k"], True),
+])
+def test_mixed_products_permuted_dense(driver, tmp_path, rng, scenario, s_dims, s_lab, d_dims, perm, d_lab,
+                                       dense_first):
+    """Mixed products whose dense operand is not in lattice order: the result
+    equals the product with the dense operand permuted first."""
+    s = rand_mia(rng, s_dims, 1500)
+    D = rng.uniform(-1, 1, int(np.prod(d_dims)))
+    write(tmp_path, "a", s)
+    (tmp_path / "D.vals").write_bytes(D.tobytes())
+    (tmp_path / "D.meta").write_text(" ".join(map(str, d_dims)) + "\n")
+    run(driver, scenario, tmp_path)
+    es = s.copy()
+    Dp = colmajor_permute(D, d_dims, perm)
+    c, _ = oracle.mixed_product(es, s_lab, Dp, [d_dims[q] for q in perm], d_lab, dense_first)
+    same(read(tmp_path, "c"), c, atol=0)
+    same(read(tmp_path, "a_after"), es, atol=0)
