@@ -388,6 +388,7 @@ struct SparseAtom;
 struct SparseExpr {
   SparseTensor t;
   Labels labels;
+  size_t inter = 0;  // trailing element-wise (inter) labels of a product result
 };
 
 // a(i, j, k): a tensor viewed with labels (MIA_Atom, MIA_Expr.h:738-1400).
@@ -551,7 +552,7 @@ inline SparseExpr nolattice_product(SparseAtom& a, SparseAtom& b, const ProductO
   SparseTensor c(dims);
   c.take(std::move(k), std::move(v));
   c.setSorted(true);  // C.setSorted(true) (SparseMIABase.h:1822)
-  return {std::move(c), std::move(labels)};
+  return {std::move(c), std::move(labels), o.l_inter.size()};
 }
 
 // MIA_Atom::operator* for the lattice case (MIA_Expr.h:864-925) -> csc_no_accum.
@@ -600,7 +601,7 @@ inline SparseExpr product(SparseAtom& a, SparseAtom& b) {
   SparseTensor c(dims);  // default sequence, sorted (SparseMIA.h:362-372)
   c.take(std::move(k), std::move(v));
   c.setSorted(true);
-  return {std::move(c), std::move(labels)};
+  return {std::move(c), std::move(labels), o.l_inter.size()};
 }
 
 }  // namespace detail
@@ -760,6 +761,7 @@ class DenseTensor {
 struct DenseExpr {
   DenseTensor t;
   Labels labels;
+  size_t inter = 0;  // trailing element-wise (inter) labels of a product result
 };
 
 struct DenseAtom {
@@ -829,7 +831,7 @@ inline DenseExpr operator*(DenseAtom a, DenseAtom b) {
     check(lnt_dense_lattice_mult_split(ad, bd, c.data(), h, w, wB, d, s, scratch(need), need, nullptr),
           "dense product");
   }
-  return {std::move(c), std::move(labels)};
+  return {std::move(c), std::move(labels), o.l_inter.size()};
 }
 
 // ---- mixed sparse / dense products ---------------------------------------------
@@ -901,7 +903,7 @@ inline SparseExpr operator*(SparseAtom a, DenseAtom b) {
   std::iota(def.begin(), def.end(), 0);
   c.change_linIdx_sequence(def);
   c.setSorted(false);
-  return {std::move(c), std::move(labels)};
+  return {std::move(c), std::move(labels), o.l_inter.size()};
 }
 
 // DenseMIA * SparseMIA: DenseLatticeBase::operator*(SparseLatticeBase)
@@ -929,7 +931,22 @@ inline SparseExpr operator*(DenseAtom a, SparseAtom b) {
   SparseTensor c(dims);
   c.take(std::move(k), std::move(v));
   c.setSorted(true);
-  return {std::move(c), std::move(labels)};
+  return {std::move(c), std::move(labels), o.l_inter.size()};
+}
+
+// MIA_Atom::operator~ (MIA_Expr.h:1376-1379, decrement_back_indices,
+// ExprUtil.h:740-766): the trailing element-wise (inter) labels of a product
+// result lose their '!', so the result can be assigned to, or combined with,
+// plain labels: d(i, l, n) = ~(a(i, j, !n) * b(j, l, !n)).
+inline SparseExpr operator~(SparseExpr e) {
+  for (size_t q = e.labels.size() - e.inter; q < e.labels.size(); ++q) e.labels[q] = !e.labels[q];
+  e.inter = 0;
+  return e;
+}
+inline DenseExpr operator~(DenseExpr e) {
+  for (size_t q = e.labels.size() - e.inter; q < e.labels.size(); ++q) e.labels[q] = !e.labels[q];
+  e.inter = 0;
+  return e;
 }
 
 template <size_t N>

@@ -6,7 +6,7 @@
 //   frontend_driver <scenario> <dir>
 // Files: <name>.keys (uint64), <name>.vals (float64), <name>.meta (text:
 // order, dims..., seq..., sorted).  Scenarios: product, product_assign,
-// elementwise, outer_inter, outer, trace, attract, merge_add, merge_sub,
+// elementwise, elementwise_decrement, outer_inter, outer, trace, attract, merge_add, merge_sub,
 // merge_self, plus_equals, sort_seq, collect, dense, dense_perm, mixed_sd,
 // mixed_sd_inter, mixed_ds, mixed_ds_inter, mixed_sd_perm, mixed_ds_perm.
 #include <cstdio>
@@ -94,6 +94,12 @@ int main(int argc, char** argv) {
       load(a, "a");
       load(b, "b");
       d(i, l, !n) = a(i, j, !n) * b(j, l, !n);
+      save(d, "c");
+    } else if (sc == "elementwise_decrement") {  // ~ turns the result's !n back into n
+      lnt::SparseNT<3> a, b, d;
+      load(a, "a");
+      load(b, "b");
+      d(i, l, n) = ~(a(i, j, !n) * b(j, l, !n));
       save(d, "c");
     } else if (sc == "outer_inter") {  // noLatticeMult: outer i, l with element-wise n
       lnt::SparseNT<2> a, b;

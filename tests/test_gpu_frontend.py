@@ -87,6 +87,18 @@ def test_elementwise_product(driver, tmp_path, rng):
     same(read(tmp_path, "c"), c)
 
 
+def test_elementwise_product_decremented(driver, tmp_path, rng):
+    """d(i,l,n) = ~(a(i,j,!n) * b(j,l,!n)): the same entries as the element-wise
+    product, assigned to a target whose n is a plain label."""
+    a = rand_mia(rng, [30, 20, 6], 800)
+    b = rand_mia(rng, [20, 25, 6], 800)
+    write(tmp_path, "a", a)
+    write(tmp_path, "b", b)
+    run(driver, "elementwise_decrement", tmp_path)
+    c, _ = oracle.product(a.copy(), ["i", "j", "!n"], b.copy(), ["j", "l", "!n"])
+    same(read(tmp_path, "c"), c)
+
+
 @pytest.mark.parametrize("scenario,a_lab,b_lab,a_dims,b_dims", [
     ("outer_inter", ["i", "!n"], ["!n", "l"], [40, 9], [9, 30]),
     ("outer", ["i", "j"], ["k", "l"], [15, 12], [12, 14]),
