@@ -162,6 +162,8 @@ class SparseTensor {
   void assign_host(const std::vector<uint64_t>& keys, const std::vector<double>& vals, bool is_sorted,
                    std::vector<int> seq = {}) {
     if (keys.size() != vals.size()) throw MIAParameterException("keys and values differ in length");
+    pk_.clear();
+    pv_.clear();
     keys_.resize(keys.size());
     vals_.resize(vals.size());
     if (!keys.empty()) {
@@ -172,6 +174,7 @@ class SparseTensor {
     sorted_ = is_sorted;
   }
   void download(std::vector<uint64_t>& keys, std::vector<double>& vals) const {
+    sync_();
     keys.resize(size());
     vals.resize(size());
     if (size()) {
@@ -186,16 +189,26 @@ class SparseTensor {
   const std::vector<int>& linIdxSequence() const { return seq_; }
   bool is_sorted() const { return sorted_; }
   void setSorted(bool s) { sorted_ = s; }
-  size_t size() const { return keys_.size(); }
+  size_t size() const { return keys_.size() + pk_.size(); }
   uint64_t dimensionality() const {
     uint64_t d = 1;
     for (auto x : dims_) d *= (uint64_t)x;
     return d;
   }
-  uint64_t* keys() { return keys_.data(); }
-  double* vals() { return vals_.data(); }
-  const uint64_t* keys() const { return keys_.data(); }
-  const double* vals() const { return vals_.data(); }
+  uint64_t* keys() { return sync_(), keys_.data(); }
+  double* vals() { return sync_(), vals_.data(); }
+  const uint64_t* keys() const { return sync_(), keys_.data(); }
+  const double* vals() const { return sync_(), vals_.data(); }
+
+  // SparseMIA::push_back (SparseMIA.h:570-578): appends one entry whose key is
+  // in this tensor's linIdxSequence; the sorted flag drops when the key is
+  // below the previous last key.  Entries wait on the host and go to the
+  // device in one copy at the next operation that reads the storage.
+  void push_back(double value, uint64_t key) {
+    if (sorted_ && size() > 0 && key < last_key_()) sorted_ = false;
+    pk_.push_back(key);
+    pv_.push_back(value);
+  }
 
   // SparseMIABase::change_linIdx_sequence (SparseMIABase.h:768-814)
   void change_linIdx_sequence(const std::vector<int>& seq) {
@@ -264,6 +277,8 @@ class SparseTensor {
 
   // internal: replace storage
   void take(DeviceBuffer<uint64_t>&& k, DeviceBuffer<double>&& v) {
+    pk_.clear();
+    pv_.clear();
     keys_ = std::move(k);
     vals_ = std::move(v);
   }
@@ -284,11 +299,37 @@ class SparseTensor {
     vals_ = std::move(v);
   }
 
+  // appends the entries staged by push_back to the device storage
+  void sync_() const {
+    if (pk_.empty()) return;
+    const size_t n = keys_.size(), m = pk_.size();
+    DeviceBuffer<uint64_t> k(n + m);
+    DeviceBuffer<double> v(n + m);
+    if (n) {
+      cuda_check(cudaMemcpy(k.data(), keys_.data(), n * 8, cudaMemcpyDeviceToDevice), "push_back");
+      cuda_check(cudaMemcpy(v.data(), vals_.data(), n * 8, cudaMemcpyDeviceToDevice), "push_back");
+    }
+    cuda_check(cudaMemcpy(k.data() + n, pk_.data(), m * 8, cudaMemcpyHostToDevice), "push_back");
+    cuda_check(cudaMemcpy(v.data() + n, pv_.data(), m * 8, cudaMemcpyHostToDevice), "push_back");
+    keys_ = std::move(k);
+    vals_ = std::move(v);
+    pk_.clear();
+    pv_.clear();
+  }
+  uint64_t last_key_() const {
+    if (!pk_.empty()) return pk_.back();
+    uint64_t h = 0;
+    cuda_check(cudaMemcpy(&h, keys_.data() + keys_.size() - 1, 8, cudaMemcpyDeviceToHost), "push_back");
+    return h;
+  }
+
   std::vector<int64_t> dims_;
   std::vector<int> seq_;
   bool sorted_ = true;  // the dims-only constructor's default (SparseMIABase.h:220)
-  DeviceBuffer<uint64_t> keys_;
-  DeviceBuffer<double> vals_;
+  mutable DeviceBuffer<uint64_t> keys_;  // mutable: staged push_back entries are appended on first read
+  mutable DeviceBuffer<double> vals_;
+  mutable std::vector<uint64_t> pk_;     // push_back entries not yet on the device
+  mutable std::vector<double> pv_;
 };
 
 // ---- expression layer ---------------------------------------------------------

@@ -6,7 +6,7 @@
 //   frontend_driver <scenario> <dir>
 // Files: <name>.keys (uint64), <name>.vals (float64), <name>.meta (text:
 // order, dims..., seq..., sorted).  Scenarios: product, product_assign,
-// elementwise, elementwise_decrement, outer_inter, outer, trace, attract, merge_add, merge_sub,
+// elementwise, elementwise_decrement, push_back, outer_inter, outer, trace, attract, merge_add, merge_sub,
 // merge_self, plus_equals, sort_seq, collect, dense, dense_perm, mixed_sd,
 // mixed_sd_inter, mixed_ds, mixed_ds_inter, mixed_sd_perm, mixed_ds_perm.
 #include <cstdio>
@@ -101,6 +101,21 @@ int main(int argc, char** argv) {
       load(b, "b");
       d(i, l, n) = ~(a(i, j, !n) * b(j, l, !n));
       save(d, "c");
+    } else if (sc == "push_back") {  // build a tensor entry by entry
+      lnt::SparseNT<3> a, b;
+      load(a, "a");
+      load(b, "b");
+      std::vector<uint64_t> k;
+      std::vector<double> v;
+      a.download(k, v);
+      lnt::SparseNT<3> t(a.dim(0), a.dim(1), a.dim(2));
+      for (size_t q = 0; q < k.size(); ++q) t.push_back(v[q], k[q]);
+      save(t, "c");
+      t.sort();
+      save(t, "c_sorted");
+      b.download(k, v);
+      for (size_t q = 0; q < k.size(); ++q) t.push_back(v[q], k[q]);
+      save(t, "c3");
     } else if (sc == "outer_inter") {  // noLatticeMult: outer i, l with element-wise n
       lnt::SparseNT<2> a, b;
       lnt::SparseNT<3> d;

@@ -276,3 +276,32 @@ def test_mixed_products_permuted_dense(driver, tmp_path, rng, scenario, s_dims, 
     c, _ = oracle.mixed_product(es, s_lab, Dp, [d_dims[q] for q in perm], d_lab, dense_first)
     same(read(tmp_path, "c"), c, atol=0)
     same(read(tmp_path, "a_after"), es, atol=0)
+
+
+@pytest.mark.parametrize("ascending", [True, False])
+def test_push_back(driver, tmp_path, rng, ascending):
+    """SparseMIA::push_back: entries kept in push order, the sorted flag
+    dropping at the first key below its predecessor; sort(); more entries
+    pushed after the storage was read (compared with the last stored key)."""
+    dims = [30, 20, 10]
+    a = rand_mia(rng, dims, 700)
+    if ascending:
+        a.keys, a.vals = oracle.sort_pairs(a.keys, a.vals)
+    b = rand_mia(rng, dims, 50)
+    write(tmp_path, "a", a)
+    write(tmp_path, "b", b)
+    run(driver, "push_back", tmp_path)
+    c = read(tmp_path, "c")
+    np.testing.assert_array_equal(c.keys, a.keys)
+    np.testing.assert_array_equal(c.vals, a.vals)
+    assert c.sorted == bool(np.all(a.keys[1:] >= a.keys[:-1]))
+    cs = read(tmp_path, "c_sorted")
+    sk, sv = oracle.sort_pairs(a.keys, a.vals)
+    np.testing.assert_array_equal(cs.keys, sk)
+    np.testing.assert_array_equal(cs.vals, sv)
+    assert cs.sorted
+    c3 = read(tmp_path, "c3")
+    allk = np.concatenate([sk, b.keys])
+    np.testing.assert_array_equal(c3.keys, allk)
+    np.testing.assert_array_equal(c3.vals, np.concatenate([sv, b.vals]))
+    assert c3.sorted == bool(np.all(allk[1:] >= allk[:-1]))
