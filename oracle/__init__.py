@@ -144,6 +144,69 @@ def lattice_mult(ak, av, h, w, d, bk, bv, wB, with_abs=False):
     return ck, cv
 
 
+def csc_times(ak, av, h, w, d, bk, bv, wB):
+    """Second oracle for the lattice product: SparseLatticeBase::csc_times
+    (SparseLatticeBase.h:2226-2351), Gustavson's column-by-column product with
+    a dense accumulator per tab.  For each column of B, its entries in row
+    order scatter A's column into the accumulator (first touch sets, later
+    ones add); every touched row is emitted, in row order.  Same pattern as
+    csc_no_accum (exact zero sums kept), different summation order."""
+    ak, bk = _u64(ak), _u64(bk)
+    av, bv = _f64(av), _f64(bv)
+    keys, vals = [], []
+    at, bt = ak // np.uint64(h * w), bk // np.uint64(w * wB)
+    for t in np.intersect1d(np.unique(at), np.unique(bt)):
+        sa, sb = at == t, bt == t
+        a_loc, a_val = ak[sa] % np.uint64(h * w), av[sa]
+        a_row, a_col = (a_loc % np.uint64(h)).astype(np.int64), (a_loc // np.uint64(h)).astype(np.int64)
+        b_loc, b_val = bk[sb] % np.uint64(w * wB), bv[sb]
+        b_row, b_col = (b_loc % np.uint64(w)).astype(np.int64), (b_loc // np.uint64(w)).astype(np.int64)
+        for c in np.unique(b_col):
+            acc, touched = {}, []
+            for k, bvv in zip(b_row[b_col == c], b_val[b_col == c]):
+                for r, avv in zip(a_row[a_col == k], a_val[a_col == k]):
+                    if r in acc:
+                        acc[r] += avv * bvv
+                    else:
+                        acc[r] = avv * bvv
+                        touched.append(r)
+            for r in sorted(touched):
+                keys.append(r + h * (c + wB * int(t)))
+                vals.append(acc[r])
+    return np.array(keys, np.uint64), np.array(vals, np.float64)
+
+
+def outer_times(ak, av, h, w, d, bk, bv, wB):
+    """Second oracle for the lattice product: SparseLatticeBase::outer_times
+    (SparseLatticeBase.h:2036-2183).  Per tab, for every inner index k present
+    in both, all products A(:,k) x B(k,:) are listed, then sorted by output key
+    and folded with collect_duplicates_function (+, zeros kept)."""
+    ak, bk = _u64(ak), _u64(bk)
+    av, bv = _f64(av), _f64(bv)
+    keys, vals = [], []
+    at, bt = ak // np.uint64(h * w), bk // np.uint64(w * wB)
+    for t in np.intersect1d(np.unique(at), np.unique(bt)):
+        sa, sb = at == t, bt == t
+        a_loc, a_val = ak[sa] % np.uint64(h * w), av[sa]
+        a_row, a_col = (a_loc % np.uint64(h)).astype(np.int64), (a_loc // np.uint64(h)).astype(np.int64)
+        b_loc, b_val = bk[sb] % np.uint64(w * wB), bv[sb]
+        b_row, b_col = (b_loc % np.uint64(w)).astype(np.int64), (b_loc // np.uint64(w)).astype(np.int64)
+        pk, pv = [], []
+        for k in np.intersect1d(a_col, b_row):
+            ia, ib = a_col == k, b_row == k
+            pk.append((a_row[ia][:, None] + h * b_col[ib][None, :]).ravel())
+            pv.append((a_val[ia][:, None] * b_val[ib][None, :]).ravel())
+        if not pk:
+            continue
+        lk, lv = sort_pairs(np.concatenate(pk).astype(np.uint64), np.concatenate(pv))
+        ck, cv = collect_duplicates(lk, lv, skip_zero_heads=False)
+        keys.append(ck + np.uint64(h * wB) * np.uint64(t))
+        vals.append(cv)
+    if not keys:
+        return np.zeros(0, np.uint64), np.zeros(0, np.float64)
+    return np.concatenate(keys), np.concatenate(vals)
+
+
 def dense_lattice_mult(A, B, h, w, wB, d) -> np.ndarray:
     """Column-major per-tab product; A (h*w*d), B (w*wB*d) flat arrays."""
     A, B = _f64(A).ravel(), _f64(B).ravel()

@@ -405,3 +405,21 @@ def test_mixed_product_vs_dense(rng, s_dims, s_lab, d_dims, d_lab, dense_first, 
     rest = np.ones(flat.size, bool)
     rest[c.keys.astype(np.int64)] = False
     assert np.all(flat[rest] == 0.0)
+
+
+
+@pytest.mark.parametrize("m1,n1,n2,p,hyper", [(20, 20, 20, 20, 1.0), (20, 20, 20, 20, 0.5), (40, 20, 20, 20, 1.0),
+                                              (20, 20, 40, 20, 0.5)])
+def test_lattice_product_second_oracles(rng, m1, n1, n2, p, hyper):
+    """sparse_lattice_mult_test_specialized.cpp:13-53: the product by
+    csc_no_accum (the oracle's restatement), csc_times and outer_times agree
+    on random lattices of ceil(p m1 hyper) / ceil(p n2 hyper) entries with
+    values U[1,10), duplicates collected: same keys, values within 1e-12."""
+    na, nb = int(np.ceil(p * m1 * hyper)), int(np.ceil(p * n2 * hyper))
+    ak = np.unique(rng.integers(0, m1 * n1 * p, na).astype(np.uint64))
+    bk = np.unique(rng.integers(0, n1 * n2 * p, nb).astype(np.uint64))
+    av, bv = rng.uniform(1, 10, ak.size), rng.uniform(1, 10, bk.size)
+    ck, cv, ca = oracle.lattice_mult(ak, av, m1, n1, p, bk, bv, n2, with_abs=True)
+    for k2, v2 in (oracle.csc_times(ak, av, m1, n1, p, bk, bv, n2), oracle.outer_times(ak, av, m1, n1, p, bk, bv, n2)):
+        np.testing.assert_array_equal(k2, ck)
+        assert np.all(np.abs(v2 - cv) <= 1e-12 * ca)
