@@ -124,25 +124,30 @@ inline uint64_t read_u64(const uint64_t* d) {
 }
 
 // ---- index labels -------------------------------------------------------------
-// An index label (MIAINDEX / NTINDEX, Index.h:28-30); !i marks it element-wise
-// (Index.h:54-57).  Each label object has its own identity.
+// An index label (MIAINDEX / NTINDEX, Index.h:28-30); each ! raises its
+// element-wise level by one (!i, !!i: Index.h:54-57, ProdInd's counter).  Each
+// label object has its own identity; products match labels by identity and
+// level, merges and assignments by identity alone (same_product_index_id,
+// Index.h:174-184).
 class Index {
  public:
-  Index() : id_(next_id()), elem_(false) {}
-  Index operator!() const { return Index(id_, !elem_); }
+  Index() : id_(next_id()), level_(0) {}
+  Index operator!() const { return Index(id_, level_ + 1); }
+  Index decremented() const { return Index(id_, level_ > 0 ? level_ - 1 : 0); }
   int id() const { return id_; }
-  bool elementwise() const { return elem_; }
-  bool operator==(const Index& o) const { return id_ == o.id_ && elem_ == o.elem_; }
+  int level() const { return level_; }
+  bool elementwise() const { return level_ > 0; }
+  bool operator==(const Index& o) const { return id_ == o.id_ && level_ == o.level_; }
   bool same_id(const Index& o) const { return id_ == o.id_; }
 
  private:
-  Index(int id, bool e) : id_(id), elem_(e) {}
+  Index(int id, int level) : id_(id), level_(level) {}
   static int next_id() {
     static std::atomic<int> n{0};
     return n++;
   }
   int id_;
-  bool elem_;
+  int level_;
 };
 using Labels = std::vector<Index>;
 
@@ -359,7 +364,7 @@ inline std::vector<int> match_order(const Labels& l, const Labels& r) {
   for (size_t i = 0; i < l.size(); ++i) {
     int pos = -1;
     for (size_t j = 0; j < r.size(); ++j)
-      if (r[j] == l[i]) pos = (int)j;
+      if (r[j].same_id(l[i])) pos = (int)j;
     if (pos < 0) throw MIAParameterException("merge operands must carry the same index labels");
     o[i] = pos;
   }
@@ -441,7 +446,9 @@ struct SparseAtom {
   // c(...) = expression: relabel only (SparseMIA::assign, SparseMIA.h:891-928)
   SparseAtom& operator=(SparseExpr&& e) {
     if (e.labels.size() != labels.size()) throw MIAParameterException("assignment between different orders");
-    if (e.labels == labels) {
+    bool same = true;  // labels match by identity, whatever their element-wise marks
+    for (size_t q = 0; q < labels.size(); ++q) same = same && labels[q].same_id(e.labels[q]);
+    if (same) {
       *m = std::move(e.t);
       return *this;
     }
@@ -651,6 +658,27 @@ inline SparseExpr operator+(SparseAtom a, SparseAtom b) { return detail::merge(a
 inline SparseExpr operator-(SparseAtom a, SparseAtom b) { return detail::merge(a, b, 1); }
 inline SparseExpr operator*(SparseAtom a, SparseAtom b) { return detail::product(a, b); }
 
+// Expressions as operands (a product or merge result feeding a further one,
+// as MIA_Atom temporaries with ownership do in the reference): the result is
+// held by an atom that owns it.
+namespace detail {
+inline SparseAtom hold(SparseExpr&& e) {
+  auto p = std::make_shared<SparseTensor>(std::move(e.t));
+  SparseAtom a{p.get(), std::move(e.labels), {}};
+  a.owned = std::move(p);
+  return a;
+}
+}  // namespace detail
+inline SparseExpr operator*(SparseExpr a, SparseAtom b) { return detail::hold(std::move(a)) * b; }
+inline SparseExpr operator*(SparseAtom a, SparseExpr b) { return a * detail::hold(std::move(b)); }
+inline SparseExpr operator*(SparseExpr a, SparseExpr b) { return detail::hold(std::move(a)) * detail::hold(std::move(b)); }
+inline SparseExpr operator+(SparseExpr a, SparseAtom b) { return detail::hold(std::move(a)) + b; }
+inline SparseExpr operator+(SparseAtom a, SparseExpr b) { return a + detail::hold(std::move(b)); }
+inline SparseExpr operator+(SparseExpr a, SparseExpr b) { return detail::hold(std::move(a)) + detail::hold(std::move(b)); }
+inline SparseExpr operator-(SparseExpr a, SparseAtom b) { return detail::hold(std::move(a)) - b; }
+inline SparseExpr operator-(SparseAtom a, SparseExpr b) { return a - detail::hold(std::move(b)); }
+inline SparseExpr operator-(SparseExpr a, SparseExpr b) { return detail::hold(std::move(a)) - detail::hold(std::move(b)); }
+
 // Destructive merges (perform_destructive_merge -> SparseMIA::merge, SparseMIA.h:1030-1060):
 // the result replaces the left operand.
 inline SparseAtom& SparseAtom::operator+=(const SparseAtom& o) {
@@ -808,10 +836,31 @@ struct DenseExpr {
 struct DenseAtom {
   DenseTensor* m;
   Labels labels;
+  // DenseMIA assignment (MIA_Atom::operator=, MIA_Expr.h:1114-1182): labels
+  // match by identity; a different label order permutes the result's modes
+  // into the target's (inplace_permute, DenseMIA.h:700-780).
   DenseAtom& operator=(DenseExpr&& e) {
-    if (e.labels != labels)
-      throw MIAParameterException("dense assignment with a different label order is not on this path");
-    *m = std::move(e.t);
+    if (e.labels.size() != labels.size()) throw MIAParameterException("assignment between different orders");
+    std::vector<int32_t> perm(labels.size());
+    bool identity = true;
+    for (size_t q = 0; q < labels.size(); ++q) {
+      int pos = -1;
+      for (size_t r = 0; r < e.labels.size(); ++r)
+        if (e.labels[r].same_id(labels[q])) pos = (int)r;
+      if (pos < 0) throw MIAParameterException("assignment with different index labels");
+      perm[q] = pos;
+      identity = identity && pos == (int)q;
+    }
+    if (identity) {
+      *m = std::move(e.t);
+      return *this;
+    }
+    std::vector<int64_t> nd;
+    for (int32_t q : perm) nd.push_back(e.t.dim(q));
+    DenseTensor out(nd);
+    check(lnt_dense_permute(e.t.data(), out.data(), (int)e.t.order(), e.t.dims().data(), perm.data(), nullptr),
+          "dense assignment");
+    *m = std::move(out);
     return *this;
   }
 };
@@ -977,15 +1026,16 @@ inline SparseExpr operator*(DenseAtom a, SparseAtom b) {
 
 // MIA_Atom::operator~ (MIA_Expr.h:1376-1379, decrement_back_indices,
 // ExprUtil.h:740-766): the trailing element-wise (inter) labels of a product
-// result lose their '!', so the result can be assigned to, or combined with,
-// plain labels: d(i, l, n) = ~(a(i, j, !n) * b(j, l, !n)).
+// result lose one '!' each, so the result can take part in a further product
+// with those indices at the lower level:
+//   c(i,k,m,n) = ~(a(i,!j,k,!l) * b(!j,!l,m,n)) * d(j,l).
 inline SparseExpr operator~(SparseExpr e) {
-  for (size_t q = e.labels.size() - e.inter; q < e.labels.size(); ++q) e.labels[q] = !e.labels[q];
+  for (size_t q = e.labels.size() - e.inter; q < e.labels.size(); ++q) e.labels[q] = e.labels[q].decremented();
   e.inter = 0;
   return e;
 }
 inline DenseExpr operator~(DenseExpr e) {
-  for (size_t q = e.labels.size() - e.inter; q < e.labels.size(); ++q) e.labels[q] = !e.labels[q];
+  for (size_t q = e.labels.size() - e.inter; q < e.labels.size(); ++q) e.labels[q] = e.labels[q].decremented();
   e.inter = 0;
   return e;
 }

@@ -265,6 +265,16 @@ def _is_elem(label: str) -> bool:
     return label.startswith("!")
 
 
+def decrement(labels, inter: int):
+    """MIA_Atom::operator~ (MIA_Expr.h:1376-1379; decrement_back_indices,
+    ExprUtil.h:740-766): the last `inter` labels lose one '!'."""
+    labels = list(labels)
+    for q in range(len(labels) - inter, len(labels)):
+        if labels[q].startswith("!"):
+            labels[q] = labels[q][1:]
+    return labels
+
+
 def product_orders(l_labels, r_labels) -> dict:
     """Mode classification of a product l(...) * r(...).
 
@@ -295,10 +305,12 @@ def product_orders(l_labels, r_labels) -> dict:
 
 def merge_index_order(l_labels, r_labels) -> list:
     """For each left label its position in the right operand
-    (pull_match_order, ExprUtil.h:511-562)."""
-    if sorted(l_labels) != sorted(r_labels):
+    (pull_match_order, ExprUtil.h:511-562), labels matched by index identity
+    whatever their element-wise marks (same_product_index_id, Index.h:174-184)."""
+    lb, rb = [_base(x) for x in l_labels], [_base(x) for x in r_labels]
+    if sorted(lb) != sorted(rb):
         raise ValueError("merge operands must carry the same labels")
-    return [r_labels.index(lab) for lab in l_labels]
+    return [rb.index(lab) for lab in lb]
 
 
 def reverse_order(order):
@@ -751,9 +763,10 @@ def assign(dest_labels, src: SparseMIA, src_labels) -> SparseMIA:
     """c(dest_labels) = <expression result with src_labels>: when the label
     orders differ only linIdxSequence and dims are rewritten, no sort
     (SparseMIA::assign, SparseMIA.h:891-928)."""
-    if list(dest_labels) == list(src_labels):
+    db, sb = [_base(x) for x in dest_labels], [_base(x) for x in src_labels]  # matched by index identity
+    if db == sb:
         return src
-    index_order = [src_labels.index(l) for l in dest_labels]
+    index_order = [sb.index(l) for l in db]
     new_dims = [src.dims[i] for i in index_order]
     lhs = reverse_order(index_order)
     new_seq = [lhs[s] for s in src.seq]

@@ -6,7 +6,8 @@
 //   frontend_driver <scenario> <dir>
 // Files: <name>.keys (uint64), <name>.vals (float64), <name>.meta (text:
 // order, dims..., seq..., sorted).  Scenarios: product, product_assign,
-// elementwise, elementwise_decrement, push_back, outer_inter, outer, trace, attract, merge_add, merge_sub,
+// elementwise, elementwise_decrement, ternary, elem_assign, repeated_elem,
+// dense_assign_perm, push_back, outer_inter, outer, trace, attract, merge_add, merge_sub,
 // merge_self, plus_equals, sort_seq, collect, dense, dense_perm, mixed_sd,
 // mixed_sd_inter, mixed_ds, mixed_ds_inter, mixed_sd_perm, mixed_ds_perm.
 #include <cstdio>
@@ -101,6 +102,34 @@ int main(int argc, char** argv) {
       load(b, "b");
       d(i, l, n) = ~(a(i, j, !n) * b(j, l, !n));
       save(d, "c");
+    } else if (sc == "ternary" || sc == "elem_assign" || sc == "repeated_elem") {
+      lnt::SparseNT<4> a, b, c;
+      lnt::SparseNT<2> b2, d2;
+      lnt::SparseNT<1> d;
+      load(a, "a");
+      load(b, "b");
+      load(b2, "b2");
+      load(d2, "d2");
+      load(d, "d");
+      if (sc == "ternary")  // sparse_mia_mult_test.cpp:147-148
+        c(i, k, m, n) = ~(a(i, !j, k, !l) * b(!j, !l, m, n)) * d2(j, l);
+      else if (sc == "elem_assign")  // :123-124
+        c(i, j, k, l) = a(i, !j, k, !l) * b2(!j, !l);
+      else  // :142-143
+        c(i, j, k, l) = ~(a(i, !j, k, !!l) * b2(!j, !!l)) * d(!l);
+      save(c, "c");
+    } else if (sc == "dense_assign_perm") {  // c(n,m,j,i) = a(i,j,k,l) * b(k,l,m,n)
+      std::ifstream meta(g_dir + "/dense.meta");
+      int64_t d1, d2;
+      int slices;
+      meta >> d1 >> d2 >> slices;
+      lnt::DenseNT<4> a(d1, d1, d2, d2), b(d2, d2, d1, d1), c(d1, d1, d1, d1);
+      a.upload(read_raw<double>(g_dir + "/A.vals"));
+      b.upload(read_raw<double>(g_dir + "/B.vals"));
+      c(n, m, j, i) = a(i, j, k, l) * b(k, l, m, n);
+      std::vector<double> hv;
+      c.download(hv);
+      write_raw(g_dir + "/C.vals", hv);
     } else if (sc == "push_back") {  // build a tensor entry by entry
       lnt::SparseNT<3> a, b;
       load(a, "a");

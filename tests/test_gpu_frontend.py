@@ -305,3 +305,47 @@ def test_push_back(driver, tmp_path, rng, ascending):
     np.testing.assert_array_equal(c3.keys, allk)
     np.testing.assert_array_equal(c3.vals, np.concatenate([sv, b.vals]))
     assert c3.sorted == bool(np.all(allk[1:] >= allk[:-1]))
+
+
+@pytest.mark.parametrize("scenario", ["ternary", "elem_assign", "repeated_elem"])
+def test_reference_mult_test_expressions(driver, tmp_path, rng, scenario):
+    """Expressions of sparse_mia_mult_test.cpp:123-148: element-wise indices
+    assigned to plain labels (matched by identity), '!!' levels, and '~' on a
+    product result feeding a further product."""
+    a = rand_mia(rng, [5, 8, 5, 8], 900)
+    b = rand_mia(rng, [8, 8, 5, 6], 900)
+    b2 = rand_mia(rng, [8, 8], 40)
+    d2 = rand_mia(rng, [8, 8], 40)
+    d = rand_mia(rng, [8], 6)
+    for name, m in (("a", a), ("b", b), ("b2", b2), ("d2", d2), ("d", d)):
+        write(tmp_path, name, m)
+    run(driver, scenario, tmp_path)
+    if scenario == "ternary":
+        t, lt = oracle.product(a.copy(), ["i", "!j", "k", "!l"], b.copy(), ["!j", "!l", "m", "n"])
+        c, lc = oracle.product(t, oracle.decrement(lt, 2), d2.copy(), ["j", "l"])
+        c = oracle.assign(["i", "k", "m", "n"], c, lc)
+    elif scenario == "elem_assign":
+        c, lc = oracle.product(a.copy(), ["i", "!j", "k", "!l"], b2.copy(), ["!j", "!l"])
+        c = oracle.assign(["i", "j", "k", "l"], c, lc)
+    else:
+        t, lt = oracle.product(a.copy(), ["i", "!j", "k", "!!l"], b2.copy(), ["!j", "!!l"])
+        c, lc = oracle.product(t, oracle.decrement(lt, 2), d.copy(), ["!l"])
+        c = oracle.assign(["i", "j", "k", "l"], c, lc)
+    same(read(tmp_path, "c"), c)
+
+
+def test_dense_assignment_permutes(driver, tmp_path, rng):
+    """c(n,m,j,i) = a(i,j,k,l) * b(k,l,m,n): the product's modes (i,j,m,n) are
+    permuted into the target's label order."""
+    d1, d2 = 6, 5
+    A = rng.uniform(-1, 1, d1 * d1 * d2 * d2)
+    B = rng.uniform(-1, 1, d2 * d2 * d1 * d1)
+    (tmp_path / "A.vals").write_bytes(A.tobytes())
+    (tmp_path / "B.vals").write_bytes(B.tobytes())
+    (tmp_path / "dense.meta").write_text(f"{d1} {d2} 0\n")
+    run(driver, "dense_assign_perm", tmp_path)
+    got = np.frombuffer((tmp_path / "C.vals").read_bytes(), np.float64)
+    An = A.reshape([d1, d1, d2, d2], order="F")
+    Bn = B.reshape([d2, d2, d1, d1], order="F")
+    ref = np.ravel(np.einsum("ijkl,klmn->nmji", An, Bn), order="F")
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-13)
