@@ -423,3 +423,52 @@ def test_lattice_product_second_oracles(rng, m1, n1, n2, p, hyper):
     for k2, v2 in (oracle.csc_times(ak, av, m1, n1, p, bk, bv, n2), oracle.outer_times(ak, av, m1, n1, p, bk, bv, n2)):
         np.testing.assert_array_equal(k2, ck)
         assert np.all(np.abs(v2 - cv) <= 1e-12 * ca)
+
+
+def _sparse_of(dense):
+    """SparseMIA of a dense array's non-zeros (default sequence, column-major keys)."""
+    flat = np.ravel(dense, order="F")
+    keys = np.flatnonzero(flat).astype(np.uint64)
+    return oracle.SparseMIA(list(dense.shape), keys, flat[keys.astype(np.int64)], sorted=True)
+
+
+def _dense_of(m):
+    keys = oracle.rekey(m.keys, m.dims, m.seq, list(range(m.order))) if m.seq != list(range(m.order)) else m.keys
+    flat = np.zeros(int(np.prod(m.dims)))
+    np.add.at(flat, keys.astype(np.int64), m.vals)
+    return flat.reshape(m.dims, order="F")
+
+
+def _thresholded(rng, shape):
+    """The reference tests' differential data: randu(0,20), entries below 15 set to 0."""
+    x = rng.uniform(0, 20, shape)
+    x[x < 15] = 0.0
+    return x
+
+
+def test_reference_mult_test_expressions_vs_dense(rng):
+    """sparse_mia_mult_test.cpp:123-148 at the oracle: element-wise results
+    assigned to plain labels (matched by identity), '~' decrementing the inter
+    labels of a product result, '!!' levels; against einsum on the dense data."""
+    A = _thresholded(rng, (5, 8, 5, 8))
+    B = _thresholded(rng, (8, 8, 5, 6))
+    B2 = _thresholded(rng, (8, 8))
+    D2 = _thresholded(rng, (8, 8))
+    D = _thresholded(rng, (8,))
+    a, b, b2, d2, d = map(_sparse_of, (A, B, B2, D2, D))
+    # c(i,j,k,l) = a(i,!j,k,!l) * b2(!j,!l)
+    c, lc = oracle.product(a.copy(), ["i", "!j", "k", "!l"], b2.copy(), ["!j", "!l"])
+    c = oracle.assign(["i", "j", "k", "l"], c, lc)
+    np.testing.assert_allclose(_dense_of(c), np.einsum("ijkl,jl->ijkl", A, B2), rtol=1e-12)
+    # c(i,k,m,n) = ~(a(i,!j,k,!l) * b(!j,!l,m,n)) * d2(j,l)
+    t, lt = oracle.product(a.copy(), ["i", "!j", "k", "!l"], b.copy(), ["!j", "!l", "m", "n"])
+    assert lt == ["i", "k", "m", "n", "!j", "!l"]
+    c, lc = oracle.product(t, oracle.decrement(lt, 2), d2.copy(), ["j", "l"])
+    c = oracle.assign(["i", "k", "m", "n"], c, lc)
+    np.testing.assert_allclose(_dense_of(c), np.einsum("ijkl,jlmn,jl->ikmn", A, B, D2), rtol=1e-12)
+    # c(i,j,k,l) = ~(a(i,!j,k,!!l) * b2(!j,!!l)) * d(!l)
+    t, lt = oracle.product(a.copy(), ["i", "!j", "k", "!!l"], b2.copy(), ["!j", "!!l"])
+    c, lc = oracle.product(t, oracle.decrement(lt, 2), d.copy(), ["!l"])
+    assert lc == ["i", "k", "j", "!l"]
+    c = oracle.assign(["i", "j", "k", "l"], c, lc)
+    np.testing.assert_allclose(_dense_of(c), np.einsum("ijkl,jl,l->ijkl", A, B2, D), rtol=1e-12)
