@@ -75,7 +75,8 @@ def load_tuned() -> dict:
     return {"sort": [], "pass8_variant": 0, "batch_chunk": 8, "tile_dense_div": 8}
 
 
-def write_header(tuned: dict):
+def render_header(tuned: dict) -> str:
+    """Text of csrc/lnt_tuned.h for the tuned values."""
     lines = [
         "// Autotuned kernel choices.  Written by libnt_b200/tune.py from timings on a",
         "// B200 (the values come from lnt_tuned.json); sort entries are tried in",
@@ -109,7 +110,11 @@ def write_header(tuned: dict):
         "}  // namespace lnt",
         "",
     ]
-    TUNED_H.write_text("\n".join(lines))
+    return "\n".join(lines)
+
+
+def write_header(tuned: dict):
+    TUNED_H.write_text(render_header(tuned))
 
 
 def _events(torch):
