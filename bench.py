@@ -44,6 +44,7 @@ WORKLOAD = ("sparse merge c(i,j,k,l)=a(i,j,k,l)+b(l,k,j,i): order-4 SparseMIA di
 IMPLEMENTATION = ("bucket histogram (A re-keyed on the fly), two 8-bit onesweep passes over the top 15 key bits, "
                   "per-bucket shared-memory sort with the duplicate fold fused")
 HBM_FALLBACK_GBS = 6650.0
+L2_NOTE = "inputs (2 GiB) and sort buffers larger than the 126 MB L2; no flush needed"
 
 
 def peaks():
@@ -205,61 +206,113 @@ def cpu_merge_sample(n_per_operand: int, seed: int = 0):
 CPU_SAMPLE = 1 << 23  # per operand: 2^24 pairs, ~1/8 of the workload
 
 
-def _reference_workers() -> int:
-    """Host cores for the reference arm: every core this process may run on, at
-    most one worker per 2 GB of available memory (a 2 x 2^23 sample peaks near
-    1.5 GB)."""
+def _host_cores() -> int:
     try:
-        cores = len(os.sched_getaffinity(0))
+        return len(os.sched_getaffinity(0))
     except AttributeError:
-        cores = os.cpu_count() or 1
-    try:
-        import psutil
-        cores = min(cores, max(1, int(psutil.virtual_memory().available // (2 << 30))))
-    except ImportError:
-        pass
-    return max(1, cores)
+        return os.cpu_count() or 1
+
+
+# ---- reference arm: the full merge per step, spread over the host cores -----
+# The reference is single-threaded (its OpenMP is commented out).  To use every
+# host core on the same workload, each step runs one complete 2 x 2^26
+# sortMerge: the reference's own re-key on slices of A, then the key range is
+# cut into one part per worker and each worker sorts its part with the
+# reference's own MSD radix sort and folds it with the restated
+# collect_duplicates.  Parts are independent (equal keys share a part), so this
+# is the same sort and fold as one sortMerge, with the top of the MSD
+# recursion's bucket split done by key range.
+_REF = {}
+
+
+def _ref_attach(folder: str, n: int):
+    import oracle
+    oracle.ref_available()
+    for name, dt in (("ak", np.uint64), ("av", np.float64), ("bk", np.uint64), ("bv", np.float64),
+                     ("ka", np.uint64)):
+        _REF[name] = np.memmap(os.path.join(folder, name), dtype=dt, mode="r+", shape=(n,))
+
+
+def _ref_rekey_slice(bounds):
+    import oracle
+    lo, hi = bounds
+    if oracle.ref_available():
+        _REF["ka"][lo:hi] = oracle.ref_rekey(_REF["ak"][lo:hi], DIMS, [0, 1, 2, 3], INDEX_ORDER)
+    else:
+        _REF["ka"][lo:hi] = oracle.rekey(_REF["ak"][lo:hi], DIMS, [0, 1, 2, 3], INDEX_ORDER)
+    return 0
+
+
+def _ref_sort_part(bounds):
+    import oracle
+    lo, hi = bounds
+    ka, bk = _REF["ka"], _REF["bk"]
+    ma = (ka >= lo) & (ka < hi)
+    mb = (bk >= lo) & (bk < hi)
+    k = np.concatenate([ka[ma], bk[mb]])
+    v = np.concatenate([_REF["av"][ma], _REF["bv"][mb]])
+    if oracle.ref_available():
+        k, v = oracle.ref_radix_sort(k, v, MAX_KEY)
+    else:
+        k, v = oracle.sort_pairs(k, v)
+    ck, _ = oracle.collect_duplicates(k, v)
+    return int(ck.size)
 
 
 def run_reference(args):
-    """The reference's own CPU path (re-key, MSD radix sort, collect) on the
-    host: the reference is single-threaded, so all host cores are used by
-    running one independent sortMerge sample per core at once (worker
-    processes); a step is one such round, the rate the samples' total pairs
-    over the round's wall time."""
+    """The reference's own CPU path (re-key, MSD radix sort, collect) for the
+    full workload on all host cores; see the comment above _REF."""
     import concurrent.futures as cf
     import multiprocessing as mp
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    import shutil
+    import tempfile
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    workers = _reference_workers()
-    # per-worker sample: 2 x 2^23 pairs up to 16 workers, smaller beyond so that a
-    # step stays near 16 x 2^24 pairs in total (at least 2 x 2^20 per worker)
-    per = CPU_SAMPLE
-    while per > (1 << 20) and per * workers > CPU_SAMPLE * 16:
-        per //= 2
-    times = []
-    kind = "port"
-    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as pool:
-        list(pool.map(_warm_worker, range(workers)))  # imports and library loads outside the timing
-        for i in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            res = list(pool.map(cpu_merge_sample, [per] * workers, [1000 * i + w for w in range(workers)]))
-            t = time.perf_counter() - t0
-            kind = res[0][1]
-            if i >= args.warmup:
-                times.append(t)
+    workers = _host_cores()
+    n = NNZ
+    folder = tempfile.mkdtemp(prefix="lnt_ref_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        rng = np.random.default_rng(4321)
+        for name in ("ak", "bk"):
+            m = np.memmap(os.path.join(folder, name), dtype=np.uint64, mode="w+", shape=(n,))
+            m[:] = rng.integers(0, MAX_KEY, n, dtype=np.uint64)
+            m.flush()
+        for name in ("av", "bv"):
+            m = np.memmap(os.path.join(folder, name), dtype=np.float64, mode="w+", shape=(n,))
+            m[:] = rng.uniform(-1, 1, n)
+            m.flush()
+        np.memmap(os.path.join(folder, "ka"), dtype=np.uint64, mode="w+", shape=(n,)).flush()
+        slices = [(n * w // workers, n * (w + 1) // workers) for w in range(workers)]
+        parts = [(MAX_KEY * w // workers, MAX_KEY * (w + 1) // workers) for w in range(workers)]
+        times = []
+        out_nnz = 0
+        import oracle
+        kind = "reference" if oracle.ref_available() else "port"
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
+                                    initializer=_ref_attach, initargs=(folder, n)) as pool:
+            list(pool.map(_warm_worker, range(workers)))  # imports and library loads outside the timing
+            for i in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                list(pool.map(_ref_rekey_slice, slices))
+                out_nnz = sum(pool.map(_ref_sort_part, parts))
+                t = time.perf_counter() - t0
+                if i >= args.warmup:
+                    times.append(t)
+    finally:
+        shutil.rmtree(folder, ignore_errors=True)
     t = statistics.median(times)
-    rate = workers * 2 * per / t
-    sample = (f"{workers} concurrent samples of 2 x 2^{per.bit_length() - 1} nnz per step (same distributions as "
-              f"the 2 x 2^26 workload), {'reference re-key + reference MSD radix sort' if kind == 'reference' else 'restated re-key + sort'}"
-              f" + restated collect_duplicates, one per worker process")
+    rate = 2 * n / t
+    sample = (f"the full workload every step: one 2 x 2^26 sortMerge, A re-keyed in {workers} slices, then "
+              f"{workers} key ranges each sorted by "
+              + ("the reference's MSD radix sort" if kind == "reference" else "the restated sort")
+              + " and folded by the restated collect_duplicates, one worker process per host core")
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "nnz/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 2 * NNZ / rate * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nnz_per_operand": NNZ,
-                       "parallelism": f"{workers} host processes, one independent merge each"},
+            "config": {"workload": WORKLOAD, "nnz_per_operand": NNZ, "l2": L2_NOTE},
+            "parallelism": f"{workers} host processes over key ranges of one merge",
+            "output_nnz": out_nnz,
             "cpu_baseline": {"value": rate, "unit": "nnz/s", "cores": workers, "kind": kind, "sample": sample},
             "e2e": {"value": rate, "unit": "nnz/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -275,6 +328,37 @@ def _warm_worker(_):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def oracle_window_check(ak, av, bk, bv, out_k, out_v, windows=4, width=1 << 24, seed=99):
+    """Checks the device merge against the oracle on key windows: the pairs of
+    A (re-keyed by the oracle) and B whose keys fall in [lo, lo + width) are
+    sorted and folded on the host, and must equal the device output's slice
+    for that range (keys exact, values within 1e-12 of the sum of |addends|).
+    The first window starts at key 0, so the position-0 rule of
+    collect_duplicates is checked as well.  Raises on a mismatch."""
+    import oracle
+    ak, av, bk, bv = (t.cpu().numpy() for t in (ak, av, bk, bv))
+    ka = oracle.rekey(ak.view(np.uint64), DIMS, [0, 1, 2, 3], INDEX_ORDER)
+    bk = bk.view(np.uint64)
+    gk = out_k.cpu().numpy().view(np.uint64)
+    gv = out_v.cpu().numpy()
+    rng = np.random.default_rng(seed)
+    los = [0] + [int(x) for x in rng.integers(1, MAX_KEY - width, windows - 1)]
+    checked = 0
+    for lo in los:
+        hi = lo + width
+        ma = (ka >= lo) & (ka < hi)
+        mb = (bk >= lo) & (bk < hi)
+        k, v = oracle.sort_pairs(np.concatenate([ka[ma], bk[mb]]), np.concatenate([av[ma], bv[mb]]))
+        ek, ev, ea = oracle.collect_duplicates(k, v, with_abs=True)
+        i0, i1 = np.searchsorted(gk, lo), np.searchsorted(gk, hi)
+        if not np.array_equal(gk[i0:i1], ek):
+            raise RuntimeError(f"merge output keys differ from the oracle in key window [{lo}, {hi})")
+        if not np.all(np.abs(gv[i0:i1] - ev) <= 1e-12 * ea):
+            raise RuntimeError(f"merge output values differ from the oracle in key window [{lo}, {hi})")
+        checked += ek.size
+    return {"windows": len(los), "window_keys": width, "output_entries_checked": checked, "ok": True}
+
+
 E2E_LANES = 3  # copy/merge streams of the end-to-end measurement
 
 
@@ -337,6 +421,7 @@ def run_ours(args):
     L.profile_reset()
     n_out = int(cnt.item())
     assert L.device_status() == 0, "device-side wait expired during timing"
+    check = oracle_window_check(ak, av, bk, bv, out_k[:n_out], out_v[:n_out]) if rank == 0 else None
 
     if args.no_e2e:
         if rank == 0:
@@ -398,7 +483,10 @@ def run_ours(args):
     e2e_ms = max_over_ranks(f0.elapsed_time(f1) / e2e_steps, world)
     e2e_value = job_throughput(n, world, e2e_ms)
     m = int(lanes[0].hcnt.item())
-    assert m == n_out and np.array_equal(lanes[0].hok[:8].numpy(), out_k[:8].cpu().numpy())
+    # the end-to-end result equals the (oracle-checked) device-resident one
+    if m != n_out or not (np.array_equal(lanes[0].hok[:m].numpy(), out_k[:m].cpu().numpy())
+                          and np.array_equal(lanes[0].hov[:m].numpy(), out_v[:m].cpu().numpy())):
+        raise RuntimeError("end-to-end merge result differs from the device-resident one")
     del lanes
     torch.cuda.empty_cache()
 
@@ -427,9 +515,10 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "nnz/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "implementation": IMPLEMENTATION, "nnz_per_operand": NNZ, "output_nnz": n_out,
-                       "l2": "inputs (2 GiB) and sort buffers larger than the 126 MB L2; no flush needed",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "config": {"workload": WORKLOAD, "nnz_per_operand": NNZ, "l2": L2_NOTE},
+            "implementation": IMPLEMENTATION, "output_nnz": n_out,
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "oracle_check": check,
             "e2e": {"value": e2e_value, "unit": "nnz/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(16 * n + 8),
                     "pipelining": f"{E2E_LANES} streams: the H2D of steps i+1, i+2 overlap step i's merge and D2H"},

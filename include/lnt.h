@@ -74,6 +74,25 @@ LNT_API uint64_t lnt_launch_count(void);
  * *detail (may be NULL) receives the raw word (which kernel gave up). */
 LNT_API int lnt_device_status(int clear, void* stream, uint32_t* detail);
 
+/* Sets the poll budget of every bounded device-side wait (the look-backs of
+ * the sort, collect, merge, scan and contraction kernels) on the current
+ * device; polls == 0 restores the default (2^24 polls, well under a minute).
+ * A wait that exhausts its budget latches its bit in the error word and
+ * continues with the partial (too small) prefix it has summed, so its kernel
+ * finishes with wrong results; lnt_device_status() then returns LNT_TIMEOUT
+ * and the results of that call must be discarded.  Synchronous; do not call
+ * it while this library's kernels run on the device.  The Python binding
+ * applies LNT_SPIN_LIMIT from the environment when it loads. */
+LNT_API int lnt_set_spin_limit(uint32_t polls);
+
+/* Runs one bounded wait on a look-back state that nothing ever publishes
+ * (the same look-back code as the collect kernels) on `stream`: it polls
+ * through the budget of lnt_set_spin_limit, latches its bit and returns, so
+ * that lnt_device_status() reports LNT_TIMEOUT afterwards.  It lets a caller
+ * check its handling of an expired wait without a fault or a hang; shorten
+ * the budget first (at the default it polls for several seconds). */
+LNT_API int lnt_diag_expired_wait(void* stream);
+
 /* Per-kernel timing: while enabled, every launch by this library is
  * bracketed by CUDA events on its own stream (a few microseconds of overhead
  * per launch; off by default). */
@@ -122,12 +141,12 @@ LNT_API int lnt_sort_variant(int index, int* bits, int* threads, int* items, int
 /* Largest pair count lnt_sort_pairs_noalloc accepts. */
 #define LNT_SORT_NOALLOC_MAX_PAIRS 262144
 
-/* lnt_sort_pairs for callers that cannot allocate device memory (a stream
- * being captured into a CUDA graph, a loop that must not synchronise on an
- * allocation, a plugin with no device allocator).  No counterpart in the
- * reference, whose sort needs no workspace.  Same result as lnt_sort_pairs,
- * out of place only (LNT_BAD_ARG if an output aliases an input); at most
- * LNT_SORT_NOALLOC_MAX_PAIRS pairs (else LNT_UNSUPPORTED).  Its scratch is one
+/* lnt_sort_pairs for callers that cannot allocate device memory (a loop that
+ * must not synchronise on an allocation, a plugin with no device allocator).
+ * No counterpart in the reference, whose sort needs no workspace.  Same
+ * result as lnt_sort_pairs, out of place only (LNT_BAD_ARG if an output range
+ * overlaps an input range or the other output); n > LNT_SORT_NOALLOC_MAX_PAIRS
+ * returns LNT_UNSUPPORTED; null pointers (n > 0) return LNT_BAD_ARG.  Its scratch is one
  * fixed 6 MiB array in device memory that every device loading this library
  * holds until exit; calls share it, so calls whose GPU work overlaps race --
  * order them on one stream.  The first call on a device looks the array up,

@@ -10,6 +10,7 @@ CPU fallback: if the library is missing, importing raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -77,6 +78,8 @@ _SIGS = {
     "lnt_version": ([], C.c_int),
     "lnt_launch_count": ([], C.c_uint64),
     "lnt_device_status": ([C.c_int, _vp, C.POINTER(C.c_uint32)], C.c_int),
+    "lnt_set_spin_limit": ([C.c_uint32], C.c_int),
+    "lnt_diag_expired_wait": ([_vp], C.c_int),
     "lnt_profile_enable": ([C.c_int], C.c_int),
     "lnt_profile_reset": ([], C.c_int),
     "lnt_profile_query": ([C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)], C.c_int),
@@ -141,6 +144,9 @@ def lib() -> C.CDLL:
             f.argtypes = args
             f.restype = res
         _lib = L
+        env = os.environ.get("LNT_SPIN_LIMIT")
+        if env:
+            set_spin_limit(int(env))
     return _lib
 
 
@@ -198,6 +204,16 @@ def device_status(clear: bool = True) -> int:
     if st not in (0, 6):
         _check(st, "lnt_device_status")
     return int(word.value)
+
+
+def set_spin_limit(polls: int = 0):
+    """Poll budget of every bounded device wait on the current device (0 = default)."""
+    _check(lib().lnt_set_spin_limit(int(polls)), "lnt_set_spin_limit")
+
+
+def diag_expired_wait():
+    """Runs one look-back wait on a state nothing publishes (lnt_diag_expired_wait)."""
+    _check(lib().lnt_diag_expired_wait(_stream()), "lnt_diag_expired_wait")
 
 
 def profile_enable(on: bool = True):

@@ -51,6 +51,7 @@ struct BucketCtrl {
   u32* status_a;     // ntiles x 256
   u32* status_b;     // ntiles x 256
   unsigned long long* bstatus;  // 2^T
+  u32* gate;         // written by the histogram: 0 = every bucket fits a CTA, 1 = take the LSD path
 };
 
 __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const PairSource src, u32 n, int T, int low_bits,
@@ -125,6 +126,7 @@ __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const PairSou
     u32 m = 0;
     for (int w = 0; w < kHistThreads / 32; ++w) m = max(m, s_w[w]);
     c.misc[0] = m;
+    *c.gate = m > (u32)kBCap ? 1u : 0u;
   }
   // digit histograms: pass A digit = bucket & (2^TA - 1), pass B digit = bucket >> TA
   const int TA = T - 8;
@@ -188,6 +190,7 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
     const u64* __restrict__ keys, const double* __restrict__ vals, BucketCtrl c, int T, int low_bits,
     int local_passes, int skip_zero_heads, u64* __restrict__ out_k, double* __restrict__ out_v,
     u64* __restrict__ d_nout) {
+  if (gated_off(c.gate, 0)) return;  // a bucket is too large: the LSD path runs instead
   extern __shared__ __align__(16) unsigned char smem[];
   u64* s_x = reinterpret_cast<u64*>(smem);                       // kSlots packed words
   double* s_v = reinterpret_cast<double*>(s_x + kSlots);         // kSlots values (input order)
@@ -203,7 +206,7 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
   __syncthreads();
   const u32 b = s_misc[0];
   const u32 start = c.start[b];
-  const u32 cnt = c.start[b + 1] - start;  // <= kBCap (checked on the host)
+  const u32 cnt = c.start[b + 1] - start;  // <= kBCap (the gate is open)
   const u64 lowmask = (1ull << low_bits) - 1ull;
   const u32 warp_base = warp * kBItems * 32;
 
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
         off += v;
         if (first_pre < first_nr) break;
         base -= first_nr;
-        if (first_nr < 32 && ++spins > kSpinLimit) {
+        if (first_nr < 32 && ++spins > spin_limit()) {
           latch_error(kErrReduceLookback);
           break;
         }
@@ -526,12 +529,12 @@ bool bucket_path_applies(size_t n, int key_bits) {
   return low >= 0 && low <= 4 * kLBits && key_bits > T;  // at most four local passes (41-bit packed words)
 }
 
-// Returns LNT_OK with *used = false when a bucket exceeds the capacity (the
-// caller then takes the LSD path).  buffers: (k1, v1) and (k0, v0), n pairs each.
+// Buffers: (k1, v1) and (k0, v0), n pairs each.  The kernels after the
+// histogram are gated on *gate == 0 (every bucket fits a CTA); the caller
+// enqueues the LSD path gated on *gate == 1.
 int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int skip_zero_heads, u64* k0, double* v0,
-                             u64* k1, double* v1, void* ctrl, u64* out_k, double* out_v, u64* d_nout,
-                             cudaStream_t s, bool* used) {
-  *used = false;
+                             u64* k1, double* v1, void* ctrl, u64* out_k, double* out_v, u64* d_nout, u32* gate,
+                             cudaStream_t s) {
   const BucketLayout L = bucket_layout(n);
   const int T = L.T, TA = T - 8, low = key_bits - T;
   unsigned char* w = static_cast<unsigned char*>(ctrl);
@@ -544,6 +547,7 @@ int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int ski
   c.status_a = reinterpret_cast<u32*>(w + L.off_sa);
   c.status_b = reinterpret_cast<u32*>(w + L.off_sb);
   c.bstatus = reinterpret_cast<unsigned long long*>(w + L.off_bstatus);
+  c.gate = gate;
   if (cudaMemsetAsync(ctrl, 0, L.total, s) != cudaSuccess) return LNT_DEVICE_ERROR;
   {
     const size_t sh = ((size_t)1 << T) * 4;
@@ -552,14 +556,13 @@ int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int ski
     bucket_hist_kernel<<<sm_count(), kHistThreads, sh, s>>>(src, n, T, low, c);
     count_launch();
   }
-  u32 maxb = 0;
-  if (cudaMemcpyAsync(&maxb, c.misc, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LNT_DEVICE_ERROR;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return LNT_DEVICE_ERROR;
-  if (maxb > (u32)kBCap) return LNT_OK;  // skewed keys: not this path
-  int st = run_onesweep_pass8(src, true, k1, v1, n, (u32)low, (1u << TA) - 1u, c.bstart_a, c.status_a, c.misc + 2, s);
+  // the bucket-size decision stays on the device: the passes below return at
+  // once when the histogram found a bucket above kBCap (skewed keys)
+  int st = run_onesweep_pass8(gated_source(src, gate, 0), true, k1, v1, n, (u32)low, (1u << TA) - 1u, c.bstart_a,
+                              c.status_a, c.misc + 2, s);
   if (st != LNT_OK) return st;
-  st = run_onesweep_pass8(plain_source(k1, v1, n), false, k0, v0, n, (u32)(low + TA), 0xFFu, c.bstart_b, c.status_b,
-                          c.misc + 3, s);
+  st = run_onesweep_pass8(gated_source(plain_source(k1, v1, n), gate, 0), false, k0, v0, n, (u32)(low + TA), 0xFFu,
+                          c.bstart_b, c.status_b, c.misc + 3, s);
   if (st != LNT_OK) return st;
   {
     const size_t sh = BucketSmem::bytes;
@@ -571,7 +574,6 @@ int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int ski
     kern<<<1u << T, kBT, sh, s>>>(k0, v0, c, T, low, local_passes, skip_zero_heads, out_k, out_v, d_nout);
     count_launch();
   }
-  *used = true;
   return launch_status();
 }
 

@@ -26,6 +26,17 @@ void register_error_reader(ErrorReader f) {
   if (g_nreaders < 64) readers()[g_nreaders++] = f;
 }
 
+static SpinLimitWriter* spin_writers() {
+  static SpinLimitWriter w[64];
+  return w;
+}
+static int g_nspin_writers = 0;
+
+void register_spin_limit_writer(SpinLimitWriter f) {
+  std::lock_guard<std::mutex> g(readers_mu());
+  if (g_nspin_writers < 64) spin_writers()[g_nspin_writers++] = f;
+}
+
 void count_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
 // ---- per-kernel event timing ----------------------------------------------
@@ -206,6 +217,14 @@ int lnt_device_status(int clear, void* stream, uint32_t* detail) {
   }
   if (detail) *detail = word;
   return word ? LNT_TIMEOUT : LNT_OK;
+}
+
+int lnt_set_spin_limit(uint32_t polls) {
+  const u32 v = polls ? polls : kSpinLimit;
+  std::lock_guard<std::mutex> g(readers_mu());
+  for (int i = 0; i < g_nspin_writers; ++i)
+    if (spin_writers()[i](v) != LNT_OK) return LNT_DEVICE_ERROR;
+  return LNT_OK;
 }
 
 int lnt_profile_enable(int on) {

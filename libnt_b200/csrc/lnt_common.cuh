@@ -49,11 +49,35 @@ static UnitErrorRegistration s_unit_error_registration;
 }  // namespace
 
 // Poll budget of every spin-wait on a flag written by another CTA.  Each poll
-// is an L2 round trip (~1 us worst case under load), so this bounds a wait at
-// well under a minute while never firing on a live predecessor.
+// is an L2 round trip (~1 us worst case under load), so the default bounds a
+// wait at well under a minute while never firing on a live predecessor.  The
+// budget is a per-unit device word (like the error word) so that
+// lnt_set_spin_limit can shorten it, e.g. to check the expiry path.
 constexpr u32 kSpinLimit = 1u << 24;
+static __device__ u32 g_lnt_spin_limit = kSpinLimit;
+
+__device__ __forceinline__ u32 spin_limit() { return *reinterpret_cast<volatile u32*>(&g_lnt_spin_limit); }
+
+typedef int (*SpinLimitWriter)(u32 polls);
+void register_spin_limit_writer(SpinLimitWriter f);
+
+namespace {
+inline int write_unit_spin_limit(u32 polls) {
+  return cudaMemcpyToSymbol(g_lnt_spin_limit, &polls, sizeof(u32)) == cudaSuccess ? LNT_OK : LNT_DEVICE_ERROR;
+}
+struct UnitSpinLimitRegistration {
+  UnitSpinLimitRegistration() { register_spin_limit_writer(&write_unit_spin_limit); }
+};
+static UnitSpinLimitRegistration s_unit_spin_limit_registration;
+}  // namespace
 
 __device__ __forceinline__ void latch_error(u32 code) { atomicOr(&g_lnt_device_error, code); }
+
+// Stream-ordered choice between two kernel sequences without a host round
+// trip: an earlier kernel on the stream writes a gate word, and a kernel
+// given (gate, want) returns at once unless *gate == want.  gate == nullptr
+// means "always run".
+__device__ __forceinline__ bool gated_off(const u32* gate, u32 want) { return gate && *gate != want; }
 
 // Launch bookkeeping (host side).
 void count_launch(int n = 1);

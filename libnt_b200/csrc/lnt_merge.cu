@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kThreads) merge_kernel(const u64* __restrict__
         off += v;
         if (first_pre < first_nr) break;
         base -= first_nr;
-        if (first_nr < 32 && ++spins > kSpinLimit) {
+        if (first_nr < 32 && ++spins > spin_limit()) {
           latch_error(kErrMergeLookback);
           break;
         }

@@ -36,11 +36,9 @@ struct LeadSummary {
   u32 full;       // the whole tile is one leading run (no new key inside)
 };
 
-__global__ void __launch_bounds__(128) lead_kernel(const u64* __restrict__ keys, const double* __restrict__ vals,
-                                                   size_t n, u32 ntiles, LeadSummary* __restrict__ lead) {
-  const int lane = threadIdx.x & 31;
-  const u32 tile = blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (tile >= ntiles) return;
+// Summary of tile `tile`'s leading run (one warp).
+__device__ __forceinline__ void lead_summary(const u64* __restrict__ keys, const double* __restrict__ vals, size_t n,
+                                             u32 tile, int lane, LeadSummary* __restrict__ lead) {
   const size_t base = (size_t)tile * kTile;
   const size_t end = min(n, base + kTile);
   LeadSummary r{0.0, 0u, 0u};
@@ -76,6 +74,15 @@ __global__ void __launch_bounds__(128) lead_kernel(const u64* __restrict__ keys,
   }
 }
 
+__global__ void __launch_bounds__(128) lead_kernel(const u64* __restrict__ keys, const double* __restrict__ vals,
+                                                   size_t n, u32 ntiles, LeadSummary* __restrict__ lead,
+                                                   const u32* gate, u32 want) {
+  if (gated_off(gate, want)) return;
+  const int lane = threadIdx.x & 31;
+  for (u32 tile = blockIdx.x * 4 + (threadIdx.x >> 5); tile < ntiles; tile += gridDim.x * 4)
+    lead_summary(keys, vals, n, tile, lane, lead);
+}
+
 __device__ __forceinline__ void st_volatile64(unsigned long long* p, unsigned long long v) {
   *reinterpret_cast<volatile unsigned long long*>(p) = v;
 }
@@ -109,7 +116,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(const unsigned long 
     excl += v;
     if (first_pre < first_nr) break;
     base -= first_nr;
-    if (first_nr < 32 && ++spins > kSpinLimit) {
+    if (first_nr < 32 && ++spins > spin_limit()) {
       latch_error(err);
       break;
     }
@@ -117,6 +124,10 @@ __device__ __forceinline__ unsigned long long warp_lookback(const unsigned long 
   return excl;
 }
 
+// PERSIST: a grid smaller than the tile count whose CTAs take tiles until
+// none is left (tiles are taken in order, so every predecessor a look-back
+// waits on belongs to a running CTA).
+template <bool PERSIST>
 __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict__ keys,
                                                            const double* __restrict__ vals, size_t n,
                                                            u32 ntiles, int skip_zero_heads,
@@ -124,7 +135,8 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
                                                            unsigned long long* __restrict__ status,
                                                            u32* __restrict__ tile_counter,
                                                            u64* __restrict__ out_k, double* __restrict__ out_v,
-                                                           u64* __restrict__ d_nout) {
+                                                           u64* __restrict__ d_nout, const u32* gate, u32 want) {
+  if (gated_off(gate, want)) return;
   __shared__ u64 s_k[kPadded];
   __shared__ double s_v[kPadded];
   __shared__ u32 s_warp[kThreads / 32];
@@ -135,9 +147,11 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
   __shared__ u32 s_tile;
   __shared__ unsigned long long s_off;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (;;) {
   if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
   __syncthreads();
   const u32 tile = s_tile;
+  if (PERSIST && tile >= ntiles) break;
   const size_t base = (size_t)tile * kTile;
   const u32 tn = (u32)min((size_t)kTile, n - base);
 #pragma unroll
@@ -307,6 +321,21 @@ __global__ void __launch_bounds__(kThreads) collect_kernel(const u64* __restrict
     __stcs(out_k + off + i, s_k[i]);
     __stcs(out_v + off + i, s_v[i]);
   }
+  if (!PERSIST) break;
+  __syncthreads();  // s_k / s_v / s_tile are reused by the next tile
+  }
+}
+
+// Look-back states of two tiles that no kernel ever publishes (zero-initialised
+// with the module).
+__device__ unsigned long long g_unpublished_status[2];
+
+// One warp of "tile 1" looks back at "tile 0", which never publishes: the
+// collect kernels' look-back spins through its poll budget, latches
+// kErrReduceLookback and returns.
+__global__ void expired_lookback_kernel() {
+  const unsigned long long off = warp_lookback(g_unpublished_status, 1u, kErrReduceLookback);
+  (void)off;
 }
 
 }  // namespace
@@ -332,8 +361,10 @@ static CollectLayout collect_layout(size_t n) {
 
 size_t collect_workspace_bytes(size_t n) { return collect_layout(n).total; }
 
-int run_collect(const u64* keys, const double* vals, size_t n, int skip_zero_heads, u64* out_k,
-                double* out_v, u64* d_nout, void* ws, cudaStream_t s) {
+// gate/want: see gated_off.  A gated call runs the persistent collect (a grid
+// of resident CTAs), so that skipping it costs a few hundred empty CTAs.
+int run_collect_gated(const u64* keys, const double* vals, size_t n, int skip_zero_heads, u64* out_k,
+                      double* out_v, u64* d_nout, void* ws, cudaStream_t s, const u32* gate, u32 want) {
   if (n == 0) {
     return cudaMemsetAsync(d_nout, 0, sizeof(u64), s) == cudaSuccess ? LNT_OK : LNT_DEVICE_ERROR;
   }
@@ -342,16 +373,33 @@ int run_collect(const u64* keys, const double* vals, size_t n, int skip_zero_hea
   // status + counter are contiguous: one memset
   if (cudaMemsetAsync(w + L.off_status, 0, L.total - L.off_status, s) != cudaSuccess) return LNT_DEVICE_ERROR;
   LeadSummary* lead = reinterpret_cast<LeadSummary*>(w + L.off_lead);
+  const u32 lead_blocks = (L.ntiles + 3) / 4;
   {
     ProfScope prof("collect_lead", s);
-    lead_kernel<<<(L.ntiles + 3) / 4, 128, 0, s>>>(keys, vals, n, L.ntiles, lead);
+    lead_kernel<<<gate ? std::min(lead_blocks, (u32)sm_count() * 8u) : lead_blocks, 128, 0, s>>>(
+        keys, vals, n, L.ntiles, lead, gate, want);
   }
+  unsigned long long* status = reinterpret_cast<unsigned long long*>(w + L.off_status);
+  u32* counter = reinterpret_cast<u32*>(w + L.off_counter);
   ProfScope prof("collect", s);
-  collect_kernel<<<L.ntiles, kThreads, 0, s>>>(keys, vals, n, L.ntiles, skip_zero_heads, lead,
-                                               reinterpret_cast<unsigned long long*>(w + L.off_status),
-                                               reinterpret_cast<u32*>(w + L.off_counter), out_k, out_v, d_nout);
+  if (gate) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, collect_kernel<true>, kThreads, 0) != cudaSuccess)
+      return LNT_DEVICE_ERROR;
+    const u32 grid = std::min(L.ntiles, (u32)(std::max(per_sm, 1) * sm_count()));
+    collect_kernel<true><<<grid, kThreads, 0, s>>>(keys, vals, n, L.ntiles, skip_zero_heads, lead, status, counter,
+                                                   out_k, out_v, d_nout, gate, want);
+  } else {
+    collect_kernel<false><<<L.ntiles, kThreads, 0, s>>>(keys, vals, n, L.ntiles, skip_zero_heads, lead, status,
+                                                        counter, out_k, out_v, d_nout, nullptr, 0);
+  }
   count_launch(2);
   return launch_status();
+}
+
+int run_collect(const u64* keys, const double* vals, size_t n, int skip_zero_heads, u64* out_k,
+                double* out_v, u64* d_nout, void* ws, cudaStream_t s) {
+  return run_collect_gated(keys, vals, n, skip_zero_heads, out_k, out_v, d_nout, ws, s, nullptr, 0);
 }
 
 }  // namespace lnt
@@ -361,7 +409,7 @@ using namespace lnt;
 namespace {
 struct SortReduceLayout {
   SortPlan plan;
-  size_t off_ctrl, off_k0, off_v0, off_k1, off_v1, off_coll, total;
+  size_t off_ctrl, off_k0, off_v0, off_k1, off_v1, off_coll, off_gate, total;
 };
 
 SortReduceLayout sort_reduce_layout(size_t n, u64 max_key) {
@@ -380,12 +428,21 @@ SortReduceLayout sort_reduce_layout(size_t n, u64 max_key) {
   off += align_up(n * 8, 256);
   L.off_coll = off;
   off += align_up(collect_workspace_bytes(n), 256);
+  L.off_gate = off;  // the bucketed path's decision word (outside every region a memset clears)
+  off += 256;
   L.total = off;
   return L;
 }
 }  // namespace
 
 extern "C" {
+
+int lnt_diag_expired_wait(void* stream) {
+  cudaStream_t s = as_stream(stream);
+  expired_lookback_kernel<<<1, 32, 0, s>>>();
+  count_launch();
+  return launch_status();
+}
 
 int lnt_collect_duplicates_workspace(size_t n, size_t* bytes) {
   if (!bytes) return LNT_BAD_ARG;
@@ -434,6 +491,9 @@ int lnt_sort_reduce(const uint64_t* a_keys, const double* a_vals, size_t na, con
   src.nb = nb;
   src.bscale = b_scale;
   src.pad = 0;
+  src.gate = nullptr;
+  src.gate_run = 0;
+  src.pad2 = 0;
   int st = make_rekey_params(a_rekey, &src.ra);
   if (st != LNT_OK) return st;
   st = make_rekey_params(b_rekey, &src.rb);
@@ -444,15 +504,21 @@ int lnt_sort_reduce(const uint64_t* a_keys, const double* a_vals, size_t na, con
   u64* k1 = reinterpret_cast<u64*>(w + L.off_k1);
   double* v1 = reinterpret_cast<double*>(w + L.off_v1);
   const int key_bits = key_bits_for(max_key);
+  // Wide keys, many pairs: the bucketed path, whose histogram decides on the
+  // device whether it can finish (every bucket fits a CTA); the LSD path is
+  // enqueued behind it gated on the opposite answer.  Nothing waits on the host.
+  const u32* gate = nullptr;
   if (bucket_path_applies(n, key_bits) && !getenv("LNT_NO_BUCKETS")) {
-    bool used = false;
+    u32* g = reinterpret_cast<u32*>(w + L.off_gate);
     st = run_bucketed_sort_reduce(src, (u32)n, key_bits, skip_zero_heads, k0, v0, k1, v1, w + L.off_ctrl,
-                                  (u64*)keys_out, vals_out, (u64*)d_nout, s, &used);
-    if (st != LNT_OK || used) return st;
+                                  (u64*)keys_out, vals_out, (u64*)d_nout, g, s);
+    if (st != LNT_OK) return st;
+    gate = g;
   }
-  st = run_sort(L.plan, src, k0, v0, k1, v1, w + L.off_ctrl, s);
+  st = run_sort(L.plan, gated_source(src, gate, 1), k0, v0, k1, v1, w + L.off_ctrl, s);
   if (st != LNT_OK) return st;
-  return run_collect(k0, v0, n, skip_zero_heads, (u64*)keys_out, vals_out, (u64*)d_nout, w + L.off_coll, s);
+  return run_collect_gated(k0, v0, n, skip_zero_heads, (u64*)keys_out, vals_out, (u64*)d_nout, w + L.off_coll, s,
+                           gate, 1);
 }
 
 }  // extern "C"

@@ -39,7 +39,7 @@ __device__ __forceinline__ unsigned long long warp_lookback(const unsigned long 
     excl += v;
     if (first_pre < first_nr) break;
     base -= first_nr;
-    if (first_nr < 32 && ++spins > kSpinLimit) {
+    if (first_nr < 32 && ++spins > spin_limit()) {
       latch_error(err);
       break;
     }

@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const PairSource src, u3
   constexpr int RADIX = 1 << BITS;
   extern __shared__ u32 sh_hist[];  // passes * RADIX
   __shared__ bool s_last;
+  if (gated_off(src.gate, src.gate_run)) return;
   for (int i = threadIdx.x; i < passes * RADIX; i += kThreads) sh_hist[i] = 0;
   __syncthreads();
   const u32 stride = gridDim.x * kThreads;
@@ -164,11 +165,16 @@ __device__ __forceinline__ u32 match_digit(u32 d) {
   return peers;
 }
 
-template <int BITS, int THREADS, int ITEMS, int W, bool FIRST>
+// PERSIST: a grid smaller than the tile count whose CTAs take tiles until
+// none is left.  Tiles are taken in order and a CTA finishes its tile before
+// taking another, so every predecessor a look-back waits on belongs to a
+// running CTA.
+template <int BITS, int THREADS, int ITEMS, int W, bool FIRST, bool PERSIST = false>
 __global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>::MINB))
     onesweep_kernel(const PairSource src, u64* __restrict__ out_k, double* __restrict__ out_v, u32 n, u32 shift,
                     u32 mask, const u32* __restrict__ bstart, u32* __restrict__ status,
                     u32* __restrict__ tile_counter) {
+  if (gated_off(src.gate, src.gate_run)) return;
   using S = OnesweepShape<BITS, THREADS, ITEMS>;
   constexpr int RADIX = S::RADIX;
   constexpr int WARPS = S::WARPS;
@@ -183,10 +189,13 @@ __global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>:
   u32* s_misc = s_glob + RADIX;                          // 16
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const u32 ntiles = (n + TILE - 1) / TILE;
+  for (;;) {
   if (tid == 0) s_misc[0] = atomicAdd(tile_counter, 1u);
   for (int i = tid; i < WARPS * RADIX; i += THREADS) s_whist[i] = 0;
   __syncthreads();
   const u32 tile = s_misc[0];
+  if (PERSIST && tile >= ntiles) break;
   const size_t tile_base = (size_t)tile * TILE;
   const u32 tile_n = (u32)min((size_t)TILE, (size_t)n - tile_base);
   const u32 warp_base = warp * ITEMS * 32;
@@ -337,7 +346,7 @@ __global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>:
           if (q < W) stalled = true;
         }
       }
-      if (stalled && ++spins > kSpinLimit) {
+      if (stalled && ++spins > spin_limit()) {
         latch_error(kErrSortLookback);
         break;
       }
@@ -353,13 +362,17 @@ __global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>:
   __syncthreads();
 
   // ---- scatter keys (digit runs -> contiguous destination ranges) ---------
+  // The clamp changes nothing in a correct run (every position is < n).  It
+  // keeps writes inside the output after a look-back gave up: a pass that
+  // reads a previous pass's partial output sees digit counts that no longer
+  // match the histogram, so its offsets could otherwise pass n.
   u32 dst[ITEMS];
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
     const u32 idx = j * THREADS + tid;
     if (idx < tile_n) {
       const u64 k = s_x[idx];
-      dst[j] = s_glob[(u32)(k >> shift) & mask] + idx;
+      dst[j] = min(s_glob[(u32)(k >> shift) & mask] + idx, n - 1u);
       __stcs(out_k + dst[j], k);
     }
   }
@@ -380,11 +393,15 @@ __global__ void __launch_bounds__(THREADS, (OnesweepShape<BITS, THREADS, ITEMS>:
     const u32 idx = j * THREADS + tid;
     if (idx < tile_n) __stcs(out_v + dst[j], reinterpret_cast<const double*>(s_x)[idx]);
   }
+  if (!PERSIST) break;
+  __syncthreads();  // shared memory is reused by the next tile
+  }
 }
 
 // Copies the (possibly re-keyed / concatenated) source into buf0 unchanged;
 // used when there is nothing to sort (all keys equal).
 __global__ void copy_source_kernel(const PairSource src, u64* __restrict__ ok, double* __restrict__ ov, u32 n) {
+  if (gated_off(src.gate, src.gate_run)) return;
   const u32 stride = gridDim.x * blockDim.x;
   for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     ok[i] = load_key<true>(src, i);
@@ -392,16 +409,15 @@ __global__ void copy_source_kernel(const PairSource src, u64* __restrict__ ok, d
   }
 }
 
-// Compiled variants: (digit bits, CTA threads, items per thread, look-back window).
-#define LNT_SORT_VARIANTS(X) \
-  X(8, 256, 16, 16)          \
-  X(8, 256, 16, 32)          \
-  X(8, 512, 8, 16)           \
-  X(8, 384, 12, 16)          \
-  X(8, 256, 12, 16)          \
-  X(9, 512, 8, 16)           \
-  X(9, 512, 8, 32)           \
-  X(9, 256, 12, 8)
+// Zeroes `words` 32-bit words (the gated form of the control block's memset).
+__global__ void zero_words_kernel(u32* __restrict__ p, size_t words, const u32* gate, u32 want) {
+  if (gated_off(gate, want)) return;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  uint4* p4 = reinterpret_cast<uint4*>(p);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words / 4; i += stride)
+    p4[i] = make_uint4(0u, 0u, 0u, 0u);
+  for (size_t i = (words / 4) * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) p[i] = 0u;
+}
 
 #define LNT_SV_ENTRY(B, T, I, W) {B, T, I, W},
 const SortVariant kVariants[] = {LNT_SORT_VARIANTS(LNT_SV_ENTRY)};
@@ -418,7 +434,15 @@ int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, d
   u32* bstart = reinterpret_cast<u32*>(c + plan.off_bstart);
   u32* status = reinterpret_cast<u32*>(c + plan.off_status);
   u32* counters = reinterpret_cast<u32*>(c + plan.off_counters);
-  if (cudaMemsetAsync(ctrl, 0, plan.ctrl_bytes, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  const bool gated = src.gate != nullptr;
+  if (gated) {  // skipped with the rest of the sort when the gate is closed
+    const size_t words = plan.ctrl_bytes / 4;  // ctrl is 256-byte aligned, ctrl_bytes a multiple of 256
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((words / 4 + 255) / 256, (size_t)sm_count() * 4));
+    zero_words_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<u32*>(ctrl), words, src.gate, src.gate_run);
+    count_launch();
+  } else if (cudaMemsetAsync(ctrl, 0, plan.ctrl_bytes, s) != cudaSuccess) {
+    return LNT_DEVICE_ERROR;
+  }
 
   // histogram of all passes
   {
@@ -438,6 +462,18 @@ int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, d
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
   cudaFuncSetAttribute(onesweep_kernel<BITS, THREADS, ITEMS, W, false>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+  u32 grid = plan.ntiles;
+  if (gated) {  // persistent grid: a closed gate then costs one wave of empty CTAs
+    cudaFuncSetAttribute(onesweep_kernel<BITS, THREADS, ITEMS, W, true, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaFuncSetAttribute(onesweep_kernel<BITS, THREADS, ITEMS, W, false, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel<BITS, THREADS, ITEMS, W, false, true>,
+                                                      THREADS, sh) != cudaSuccess)
+      return LNT_DEVICE_ERROR;
+    grid = std::min(grid, (u32)(std::max(per_sm, 1) * sm_count()));
+  }
   const u64* in_k = nullptr;
   const double* in_v = nullptr;
   for (int p = 0; p < plan.passes; ++p) {
@@ -450,12 +486,20 @@ int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, d
     u32* st = status + (size_t)p * plan.ntiles * RADIX;
     ProfScope prof("sort_onesweep", s);
     if (p == 0) {
-      onesweep_kernel<BITS, THREADS, ITEMS, W, true><<<plan.ntiles, THREADS, sh, s>>>(
-          src, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
+      if (gated)
+        onesweep_kernel<BITS, THREADS, ITEMS, W, true, true><<<grid, THREADS, sh, s>>>(
+            src, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
+      else
+        onesweep_kernel<BITS, THREADS, ITEMS, W, true><<<grid, THREADS, sh, s>>>(
+            src, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
     } else {
-      const PairSource ps = plain_source(in_k, in_v, plan.n);
-      onesweep_kernel<BITS, THREADS, ITEMS, W, false><<<plan.ntiles, THREADS, sh, s>>>(
-          ps, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
+      const PairSource ps = gated_source(plain_source(in_k, in_v, plan.n), src.gate, src.gate_run);
+      if (gated)
+        onesweep_kernel<BITS, THREADS, ITEMS, W, false, true><<<grid, THREADS, sh, s>>>(
+            ps, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
+      else
+        onesweep_kernel<BITS, THREADS, ITEMS, W, false><<<grid, THREADS, sh, s>>>(
+            ps, ok, ov, plan.n, (u32)shift, mask, bstart + p * RADIX, st, counters + p);
     }
     count_launch();
     in_k = ok;

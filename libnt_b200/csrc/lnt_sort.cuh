@@ -34,6 +34,11 @@ struct PairSource {
   int pad;
   RekeyParams ra;
   RekeyParams rb;
+  // Kernels reading this source run only when gate == nullptr or
+  // *gate == gate_run (see gated_off); a gated sort uses persistent grids.
+  const u32* gate;
+  u32 gate_run;
+  u32 pad2;
 };
 
 // Host: single-array source (no re-key).
@@ -49,8 +54,30 @@ inline PairSource plain_source(const u64* k, const double* v, size_t n) {
   s.pad = 0;
   s.ra.order = 0;
   s.rb.order = 0;
+  s.gate = nullptr;
+  s.gate_run = 0;
+  s.pad2 = 0;
   return s;
 }
+
+// The same source, gated on (gate, run).
+inline PairSource gated_source(PairSource s, const u32* gate, u32 run) {
+  s.gate = gate;
+  s.gate_run = run;
+  return s;
+}
+
+// Compiled onesweep variants: (digit bits, CTA threads, items per thread,
+// look-back window).  The autotuner's variant indices follow this order.
+#define LNT_SORT_VARIANTS(X) \
+  X(8, 256, 16, 16)          \
+  X(8, 256, 16, 32)          \
+  X(8, 512, 8, 16)           \
+  X(8, 384, 12, 16)          \
+  X(8, 256, 12, 16)          \
+  X(9, 512, 8, 16)           \
+  X(9, 512, 8, 32)           \
+  X(9, 256, 12, 8)
 
 // One compiled onesweep variant.
 struct SortVariant {
@@ -101,8 +128,16 @@ int run_onesweep_pass8(const PairSource& src, bool first, u64* out_k, double* ou
 // keys have at most 28 bits below the bucket bits.
 bool bucket_path_applies(size_t n, int key_bits);
 size_t bucket_ctrl_bytes(size_t n);
+// Enqueues the bucketed path.  Its histogram kernel writes *gate: 0 when every
+// bucket fits a CTA (the path's remaining kernels run), 1 when one does not
+// (they return at once, and the caller's LSD path, gated on 1, runs instead).
+// No host synchronisation.
 int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int skip_zero_heads, u64* k0, double* v0,
-                             u64* k1, double* v1, void* ctrl, u64* out_k, double* out_v, u64* d_nout,
-                             cudaStream_t s, bool* used);
+                             u64* k1, double* v1, void* ctrl, u64* out_k, double* out_v, u64* d_nout, u32* gate,
+                             cudaStream_t s);
+
+// Duplicate collection gated on (gate, want); persistent grid when gated.
+int run_collect_gated(const u64* keys, const double* vals, size_t n, int skip_zero_heads, u64* out_k,
+                      double* out_v, u64* d_nout, void* ws, cudaStream_t s, const u32* gate, u32 want);
 
 }  // namespace lnt
