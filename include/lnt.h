@@ -383,12 +383,23 @@ LNT_API int lnt_dense_lattice_mult_split(const double* A, const double* B, doubl
 
 /* _crt: float64 operands rounded to beta-bit integers per row of A / column of
  * B (power-of-two scaled), products computed exactly modulo `moduli` pairwise
- * coprime integers <= 256 as INT8 tensor-core GEMMs with INT32 accumulation,
- * and reconstructed by Chinese remaindering in double-double;
+ * coprime integers <= 256 as INT8 tensor-core GEMMs (tcgen05) with INT32
+ * accumulation, each product reduced modulo its modulus in the GEMM's
+ * epilogue, and reconstructed by Chinese remaindering in exact integers;
  * beta = min(floor((log2 prod(moduli) - log2 w - 3) / 2), 53), error about
  * 2^(2-beta) |A||B| per entry (13 moduli: beta = 42 at w = 16384; 16 moduli:
  * beta = 53).  Requires w < 2^17 and 2 <= moduli <= 20. */
 LNT_API int lnt_dense_crt_workspace(int64_t h, int64_t w, int64_t wB, int moduli, size_t* bytes);
+/* The number of moduli for _crt that keeps every entry's error within
+ * tol * (|A||B|)_ij (tol = 1e-12 for float64-class results): the error grows
+ * with the largest ratio R of a row's (A) or column's (B) maximum magnitude
+ * to its mean magnitude, which one pass over A and B measures here; the count
+ * is the smallest with beta >= 2 + log2 R + log2(1/tol) (uniform data, R ~ 2:
+ * 14 moduli at w = 16384, 13 at w = 4096; mantissas times 2^+-20, R ~ 30: 15
+ * at w = 16384).  Synchronous on `stream` (the count is returned to the host);
+ * workspace of at least 16 h + 768 bytes, 256-byte aligned. */
+LNT_API int lnt_dense_crt_moduli(const double* A, const double* B, int64_t h, int64_t w, int64_t wB, int64_t d,
+                                 double tol, void* workspace, size_t workspace_bytes, int* moduli, void* stream);
 LNT_API int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int64_t h,
                                        int64_t w, int64_t wB, int64_t d, int moduli,
                                        void* workspace, size_t workspace_bytes, void* stream);

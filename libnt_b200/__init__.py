@@ -124,6 +124,8 @@ _SIGS = {
     "lnt_dense_lattice_mult_split": ([_vp, _vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, _vp,
                                       _sz, _vp], C.c_int),
     "lnt_dense_crt_workspace": ([C.c_int64, C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_size_t)], C.c_int),
+    "lnt_dense_crt_moduli": ([_vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_double, _vp, _sz,
+                              C.POINTER(C.c_int), _vp], C.c_int),
     "lnt_dense_lattice_mult_crt": ([_vp, _vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int, _vp,
                                     _sz, _vp], C.c_int),
 }
@@ -535,6 +537,15 @@ def dense_crt_workspace(h: int, w: int, wB: int, moduli: int = 13) -> int:
     b = C.c_size_t(0)
     _check(lib().lnt_dense_crt_workspace(h, w, wB, moduli, C.byref(b)), "lnt_dense_crt_workspace")
     return b.value
+
+
+def dense_crt_moduli(A, B, h: int, w: int, wB: int, d: int = 1, tol: float = 1e-12) -> int:
+    """Moduli count for dense_mult_crt within tol * |A||B| per entry (lnt_dense_crt_moduli)."""
+    ws = workspace(16 * h + 768, A.device)
+    m = C.c_int(0)
+    _check(lib().lnt_dense_crt_moduli(_ptr(A), _ptr(B), h, w, wB, d, float(tol), _ptr(ws), ws.numel(), C.byref(m),
+                                      _stream()), "lnt_dense_crt_moduli")
+    return int(m.value)
 
 
 def dense_permute(x, dims, perm):

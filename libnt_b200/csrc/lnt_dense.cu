@@ -1,11 +1,15 @@
 // Dense lattice product C(:,:,t) = A(:,:,t) * B(:,:,t), column-major float64
 // (the reference's DenseLatticeBase::operator*, DenseLatticeBase.h:404-430: an
-// Eigen GEMM per tab), two ways:
+// Eigen GEMM per tab), three ways:
 //
-// lnt_dense_lattice_mult_fp64: plain FP64 GEMM per tab (cuBLASLt DGEMM).
+// lnt_dense_lattice_mult_fp64: plain FP64 GEMM per tab (cuBLASLt DGEMM), the
+// comparator of the emulated products.
+//
+// lnt_dense_lattice_mult_crt (scheme II below): the products on the INT8
+// tensor cores through this library's own tcgen05 GEMM (lnt_modgemm.cu).
 //
 // lnt_dense_lattice_mult_split: error-free splitting onto the integer tensor
-// cores (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix
+// cores (its INT8 GEMMs are cuBLASLt library GEMMs) (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix
 // multiplication by using fast routines of matrix multiplication and its
 // applications", Numer. Algorithms 59 (2012), scheme I with integer slices):
 //   1. each row of A and each column of B is scaled by a power of two so its
@@ -29,11 +33,16 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 
 #include "lnt_common.cuh"
 
 namespace lnt {
+
+int run_mod_gemm(const signed char* ra, const signed char* rb, int nmod, const int* moduli, u64 Mp, u64 Np, u64 Kp,
+                 unsigned char* out, cudaStream_t s);
+
 namespace {
 
 constexpr int kDigitBits = 7;
@@ -268,10 +277,12 @@ int lt_dgemm(const double* A, const double* B, double* C, u64 m, u64 n, u64 k, v
 //      integers A', B' of at most beta bits (|A'| <= 2^(beta-1));
 //   2. for each modulus m_l (pairwise coprime, <= 256) the symmetric residues
 //      A' mod m_l, B' mod m_l fit INT8 and P_l = (A' mod m_l)(B' mod m_l) is an
-//      exact INT8 tensor-core GEMM with INT32 accumulation (|P_l| <= 2^14 K);
-//   3. per entry, y_l = (P_l mod m_l) * ((M/m_l)^-1 mod m_l) mod m_l and
-//      S = sum_l y_l / m_l in double-double; A'B' = M (S - round(S)) exactly as
-//      long as |A'B'| < M/2 (M = prod m_l), which fixes beta:
+//      exact INT8 tensor-core GEMM with INT32 accumulation (|P_l| <= 2^14 K),
+//      run by the hand-written tcgen05 kernel of lnt_modgemm.cu, whose
+//      epilogue stores only r_l = P_l mod m_l (one byte per entry);
+//   3. per entry, X = sum_l r_l (M/m_l) ((M/m_l)^-1 mod m_l) reduced modulo M
+//      into (-M/2, M/2] in exact integer limbs is A'B', as long as
+//      |A'B'| < M/2 (M = prod m_l), which fixes beta:
 //      2 beta <= log2 M - log2 K - 3.
 // The error is the rounding of A and B to beta bits: about 2^(2-beta) |A||B|
 // componentwise; N moduli give beta = floor((log2 M - log2 K - 3) / 2).
@@ -440,67 +451,132 @@ __global__ void residue_b_kernel(const double* __restrict__ B, u64 w, u64 wB, u6
   }
 }
 
-// Chinese remaindering of the P.n INT32 products, exact in integers, scaled
-// back to float64.  Per entry: T = sum_l p_l V_l as LV+1 signed 64-bit limb
-// sums (27-bit limbs; |p_l| < 2^31 so each sum stays below 2^63), carried into
-// normalised limbs; q = round(T / M) from a double estimate, exact because
-// A'B' = T - q M satisfies |A'B'| <= M/32 (the choice of beta) while the
-// estimate errs by under 2^-15; X = T - q M in limbs, converted to double
-// once (Horner from the top limb).  Grid: x over rows of C (coalesced), y over
-// columns.
+// Chinese remaindering of the residues r_l = (A'B' mod m_l) in [0, m_l), exact
+// in integers, scaled back to float64.  Per entry: T = sum_l r_l V_l as LV+1
+// signed 64-bit limb sums (27-bit limbs; r_l < 2^8, so each sum stays far
+// below 2^63), carried into normalised limbs; q = round(T / M) from a double
+// estimate, exact because A'B' = T - q M satisfies |A'B'| <= M/32 (the choice
+// of beta) while the estimate errs by under 2^-15; X = T - q M in limbs,
+// converted to double once (Horner from the top limb).  Each thread takes four
+// consecutive rows (one 4-byte load per modulus); grid x over rows of C, y
+// over columns.
 template <int LV>
-__global__ void __launch_bounds__(256) crt_kernel(const int* __restrict__ prod, u64 Mp, u64 Np, u64 h, u64 wB,
-                                                  CrtParams P, const int* __restrict__ eA,
+__global__ void __launch_bounds__(256) crt_kernel(const unsigned char* __restrict__ res, u64 Mp, u64 Np, u64 h,
+                                                  u64 wB, CrtParams P, const int* __restrict__ eA,
                                                   const int* __restrict__ eB, double* __restrict__ C) {
-  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= h) return;
+  const u64 i0 = ((u64)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (i0 >= h) return;  // Mp is a multiple of 16: rows i0 .. i0+3 lie inside every plane
   const u64 plane = Mp * Np;
-  const int ea = eA[i] - 2 * P.beta;
+  int ea[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) ea[c] = i0 + c < h ? eA[i0 + c] - 2 * P.beta : 0;
   constexpr long long kMask = (1ll << kLimbBits) - 1;
   constexpr double kRadix = (double)(1ll << kLimbBits);
   for (u64 j = blockIdx.y; j < wB; j += gridDim.y) {
-    const u64 src = i + Mp * j;
-    long long acc[LV + 1];
+    long long acc[4][LV + 1];
 #pragma unroll
-    for (int b = 0; b <= LV; ++b) acc[b] = 0;
-#pragma unroll 4
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+      for (int b = 0; b <= LV; ++b) acc[c][b] = 0;
+    const unsigned char* src = res + i0 + Mp * j;
+#pragma unroll 2
     for (int l = 0; l < P.n; ++l) {
-      const int pl = __ldcs(prod + (u64)l * plane + src);
+      const u32 w4 = __ldcs(reinterpret_cast<const u32*>(src + (u64)l * plane));
 #pragma unroll
-      for (int b = 0; b < LV; ++b) acc[b] += (long long)pl * (int)P.V[l][b];  // 32 x 32 -> 64
+      for (int b = 0; b < LV; ++b) {
+        const u32 v = P.V[l][b];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[c][b] += (long long)((w4 >> (8 * c)) & 0xffu) * v;
+      }
     }
 #pragma unroll
-    for (int b = 0; b < LV; ++b) {  // normalise: limbs in [0, 2^27), the top one signed
-      const long long c = acc[b] >> kLimbBits;
-      acc[b] &= kMask;
-      acc[b + 1] += c;
+    for (int c = 0; c < 4; ++c) {
+      if (i0 + c >= h) break;
+      long long* a = acc[c];
+#pragma unroll
+      for (int b = 0; b < LV; ++b) {  // normalise: limbs in [0, 2^27), the top one signed
+        const long long cy = a[b] >> kLimbBits;
+        a[b] &= kMask;
+        a[b + 1] += cy;
+      }
+      double td = (double)a[LV];
+#pragma unroll
+      for (int b = LV - 1; b >= 0; --b) td = fma(td, kRadix, (double)a[b]);
+      const long long q = __double2ll_rn(td * P.Minv);
+      const int qlo = (int)(q & kMask), qhi = (int)(q >> kLimbBits);  // |q| < 2^36
+#pragma unroll
+      for (int b = 0; b < LV; ++b) {
+        a[b] -= (long long)qlo * (int)P.Ml[b];
+        a[b + 1] -= (long long)qhi * (int)P.Ml[b];
+      }
+#pragma unroll
+      for (int b = 0; b < LV; ++b) {
+        const long long cy = a[b] >> kLimbBits;
+        a[b] &= kMask;
+        a[b + 1] += cy;
+      }
+      double x = (double)a[LV];
+#pragma unroll
+      for (int b = LV - 1; b >= 0; --b) x = fma(x, kRadix, (double)a[b]);
+      C[i0 + c + h * j] = scale2(x, ea[c] + eB[j]);
     }
-    double td = (double)acc[LV];
-#pragma unroll
-    for (int b = LV - 1; b >= 0; --b) td = fma(td, kRadix, (double)acc[b]);
-    const long long q = __double2ll_rn(td * P.Minv);
-    const int qlo = (int)(q & kMask), qhi = (int)(q >> kLimbBits);  // |q| < 2^36
-#pragma unroll
-    for (int b = 0; b < LV; ++b) {
-      acc[b] -= (long long)qlo * (int)P.Ml[b];
-      acc[b + 1] -= (long long)qhi * (int)P.Ml[b];
-    }
-#pragma unroll
-    for (int b = 0; b < LV; ++b) {
-      const long long c = acc[b] >> kLimbBits;
-      acc[b] &= kMask;
-      acc[b + 1] += c;
-    }
-    double x = (double)acc[LV];
-#pragma unroll
-    for (int b = LV - 1; b >= 0; --b) x = fma(x, kRadix, (double)acc[b]);
-    C[i + h * j] = scale2(x, ea + eB[j]);
   }
+}
+
+// ---- choosing the number of moduli ------------------------------------------
+// The rounding of A and B to beta-bit integers per row / column bounds the
+// error of entry (i, j) by about 2^(1-beta) (max_k |a_ik| sum_k |b_kj| +
+// sum_k |a_ik| max_k |b_kj|), so relative to (|A||B|)_ij it grows with the
+// ratio of each row's (column's) largest magnitude to its mean magnitude.
+// These kernels find the largest such ratio over the rows of A and the
+// columns of B (all-zero rows and columns excluded).
+
+// Per-row max |a| (as ordered bit patterns) and sum |a| over a chunk of columns.
+__global__ void row_absstat_kernel(const double* __restrict__ A, u64 h, u64 w, u64 kchunk,
+                                   unsigned long long* __restrict__ rmax, double* __restrict__ rsum) {
+  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= h) return;
+  const u64 k0 = (u64)blockIdx.y * kchunk, k1 = min(w, k0 + kchunk);
+  double m = 0.0, sm = 0.0;
+  for (u64 k = k0; k < k1; ++k) {
+    const double x = fabs(A[i + h * k]);
+    m = fmax(m, x);
+    sm += x;
+  }
+  atomicMax(&rmax[i], (unsigned long long)__double_as_longlong(m));  // non-negative: bit order = value order
+  atomicAdd(&rsum[i], sm);
+}
+
+__global__ void row_ratio_kernel(const unsigned long long* __restrict__ rmax, const double* __restrict__ rsum, u64 h,
+                                 u64 w, unsigned long long* __restrict__ out) {
+  const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= h || !(rsum[i] > 0.0)) return;
+  const double r = __longlong_as_double((long long)rmax[i]) * (double)w / rsum[i];
+  atomicMax(out, (unsigned long long)__double_as_longlong(r));
+}
+
+// One warp per column of B (w x wB, col-major): max / mean of |b|.
+__global__ void col_ratio_kernel(const double* __restrict__ B, u64 w, u64 wB, unsigned long long* __restrict__ out) {
+  const u64 j = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= wB) return;
+  double m = 0.0, sm = 0.0;
+  for (u64 k = lane; k < w; k += 32) {
+    const double x = fabs(B[k + w * j]);
+    m = fmax(m, x);
+    sm += x;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    sm += __shfl_xor_sync(0xffffffffu, sm, o);
+  }
+  if (lane == 0 && sm > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m * (double)w / sm));
 }
 
 struct CrtLayout {
   u64 Kp, Mp, Np;
-  size_t off_ea, off_eb, off_ra, off_rb, off_prod, off_lt, lt_bytes, total;
+  size_t off_ea, off_eb, off_ra, off_rb, off_prod, total;
 };
 
 CrtLayout crt_layout(u64 h, u64 w, u64 wB, int n) {
@@ -517,11 +593,8 @@ CrtLayout crt_layout(u64 h, u64 w, u64 wB, int n) {
   off += align_up((u64)n * L.Mp * L.Kp, 256);
   L.off_rb = off;
   off += align_up((u64)n * L.Np * L.Kp, 256);
-  L.off_prod = off;
-  off += align_up((u64)n * L.Mp * L.Np * 4, 256);
-  L.lt_bytes = 64ull << 20;
-  L.off_lt = off;
-  off += L.lt_bytes;
+  L.off_prod = off;  // residues of the products: n planes of Mp x Np bytes
+  off += align_up((u64)n * L.Mp * L.Np, 256);
   L.total = off;
   return L;
 }
@@ -689,6 +762,48 @@ int lnt_dense_lattice_mult_split(const double* A, const double* B, double* C, in
 }
 
 
+int lnt_dense_crt_moduli(const double* A, const double* B, int64_t h, int64_t w, int64_t wB, int64_t d, double tol,
+                         void* workspace, size_t workspace_bytes, int* moduli, void* stream) {
+  int st = check_dense(h, w, wB, d);
+  if (st != LNT_OK) return st;
+  if (!A || !B || !moduli || !(tol > 0.0)) return LNT_BAD_ARG;
+  const size_t need = align_up((size_t)h * 8, 256) * 2 + 256;
+  if (!workspace || workspace_bytes < need || (uintptr_t)workspace % 256) return LNT_WORKSPACE;
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  auto* rmax = reinterpret_cast<unsigned long long*>(ws);
+  auto* rsum = reinterpret_cast<double*>(ws + align_up((size_t)h * 8, 256));
+  auto* out = reinterpret_cast<unsigned long long*>(ws + 2 * align_up((size_t)h * 8, 256));
+  cudaStream_t s = as_stream(stream);
+  const u64 uh = h, uw = w, uwB = wB, kchunk = 256;
+  if (cudaMemsetAsync(out, 0, 8, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  for (int64_t t = 0; t < d; ++t) {
+    if (cudaMemsetAsync(ws, 0, 2 * align_up((size_t)h * 8, 256), s) != cudaSuccess) return LNT_DEVICE_ERROR;
+    row_absstat_kernel<<<dim3((unsigned)((uh + 255) / 256), (unsigned)((uw + kchunk - 1) / kchunk)), 256, 0, s>>>(
+        A + (u64)t * uh * uw, uh, uw, kchunk, rmax, rsum);
+    row_ratio_kernel<<<(unsigned)((uh + 255) / 256), 256, 0, s>>>(rmax, rsum, uh, uw, out);
+    col_ratio_kernel<<<(unsigned)((uwB * 32 + 255) / 256), 256, 0, s>>>(B + (u64)t * uw * uwB, uw, uwB, out);
+    count_launch(3);
+  }
+  unsigned long long bits = 0;
+  if (cudaMemcpyAsync(&bits, out, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return LNT_DEVICE_ERROR;
+  double ratio = 0.0;
+  std::memcpy(&ratio, &bits, 8);
+  // |error_ij| <= 2^(1-beta) (max_k|a_ik| sum_k|b_kj| + sum_k|a_ik| max_k|b_kj|)
+  //            <~ 2^(2-beta) R (|A||B|)_ij, with R the largest max / mean ratio
+  const double lr = ratio > 1.0 ? std::log2(ratio) : 0.0;
+  const int need_beta = (int)std::ceil(2.0 + lr - std::log2(tol));
+  for (int n = 2; n <= kMaxModuli; ++n) {
+    CrtParams P;
+    if (make_crt_params(n, (u64)w, &P) == LNT_OK && P.beta >= std::min(need_beta, 53)) {
+      *moduli = n;
+      return LNT_OK;
+    }
+  }
+  *moduli = kMaxModuli;
+  return LNT_OK;
+}
+
 int lnt_dense_crt_workspace(int64_t h, int64_t w, int64_t wB, int moduli, size_t* bytes) {
   int st = check_dense(h, w, wB, 1);
   if (st != LNT_OK) return st;
@@ -719,7 +834,7 @@ int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int6
   int* eB = reinterpret_cast<int*>(ws + L.off_eb);
   signed char* ra = reinterpret_cast<signed char*>(ws + L.off_ra);
   signed char* rb = reinterpret_cast<signed char*>(ws + L.off_rb);
-  int* prod = reinterpret_cast<int*>(ws + L.off_prod);
+  unsigned char* prod = ws + L.off_prod;
   cudaStream_t s = as_stream(stream);
   const int sms = sm_count();
   const u64 uh = h, uw = w, uwB = wB, Kp = L.Kp;
@@ -745,16 +860,15 @@ int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int6
       residue_b_kernel<<<dim3(gx, gyb), 256, 0, s>>>(Bt, uw, uwB, L.Np, Kp, eB, P, rb);
       count_launch(5);
     }
-    for (int l = 0; l < moduli; ++l) {
-      st = lt_int8_gemm(ra + (u64)l * L.Mp * Kp, (int)Kp, rb + (u64)l * L.Np * Kp, (int)Kp,
-                        prod + (u64)l * L.Mp * L.Np, L.Mp, L.Np, Kp, ws + L.off_lt, L.lt_bytes, s);
-      if (st != LNT_OK) return st;
-      count_launch();
-    }
+    // all moduli's products on the tensor cores, reduced modulo m_l in the epilogue
+    st = run_mod_gemm(ra, rb, moduli, P.m, L.Mp, L.Np, Kp, prod, s);
+    if (st != LNT_OK) return st;
     {
       ProfScope prof("dense_crt", s);
-      const unsigned gy = (unsigned)std::min<u64>(uwB, std::max<u64>(1, (u64)sms * 32 / ((uh + 255) / 256)));
-      const dim3 grid((unsigned)((uh + 255) / 256), gy);
+      const u64 rows4 = (uh + 3) / 4;
+      const unsigned gx = (unsigned)((rows4 + 255) / 256);
+      const unsigned gy = (unsigned)std::min<u64>(uwB, std::max<u64>(1, (u64)sms * 32 / gx));
+      const dim3 grid(gx, gy);
       switch (P.lv) {
         case 1:
         case 2:

@@ -793,8 +793,14 @@ using SparseMIA = SparseNT<N>;
 
 // ---- dense tensors -------------------------------------------------------------
 // Column-major dense multi-index array (DenseMIA<double, N>); products run as
-// lattice products (DenseLatticeBase::operator*), in float64 or split
-// precision (INT8 tensor-core slices, error about 2^(1-7s) |A||B|).
+// lattice products (DenseLatticeBase::operator*).  By default they are
+// float64-class products emulated on the INT8 tensor cores (Ozaki scheme II,
+// lnt_dense_lattice_mult_crt): every entry of C is within 1e-12 of
+// (|A||B|)_ij -- the error metric is relative to the product of magnitudes,
+// not to |C_ij|, which cancellation can make arbitrarily small -- with the
+// number of moduli chosen from the operands (lnt_dense_crt_moduli).
+// precision() = Precision::Float64 selects the plain float64 GEMM, slices() > 0
+// the scheme I slices (error about 2^(1-7s) |A||B|).
 class DenseTensor {
  public:
   DenseTensor() = default;
@@ -817,7 +823,12 @@ class DenseTensor {
     h.resize(numel());
     cuda_check(cudaMemcpy(h.data(), data(), h.size() * 8, cudaMemcpyDeviceToHost), "download");
   }
-  static int& slices() {  // 0: plain float64 products; 5..8: split precision
+  enum class Precision { Emulated, Float64 };
+  static Precision& precision() {  // Emulated (default): scheme II within 1e-12 of |A||B|
+    thread_local Precision p = Precision::Emulated;
+    return p;
+  }
+  static int& slices() {  // > 0 (5..8): scheme I with that many slices, overriding precision()
     thread_local int s = 0;
     return s;
   }
@@ -910,15 +921,24 @@ inline DenseExpr operator*(DenseAtom a, DenseAtom b) {
   for (int i : o.l_inter) dims.push_back(a.m->dim(i)), labels.push_back(a.labels[i]);
   DenseTensor c(dims);
   const int s = DenseTensor::slices();
-  if (s == 0) {
+  if (s > 0) {
     size_t need = 0;
+    check(lnt_dense_split_workspace(h, w, wB, s, &need), "dense product");
+    check(lnt_dense_lattice_mult_split(ad, bd, c.data(), h, w, wB, d, s, scratch(need), need, nullptr),
+          "dense product");
+  } else if (DenseTensor::precision() == DenseTensor::Precision::Float64 || w >= (int64_t{1} << 17)) {
+    size_t need = 0;  // (scheme II needs w < 2^17: INT32 exactness of the residue products)
     check(lnt_dense_fp64_workspace(&need), "dense product");
     check(lnt_dense_lattice_mult_fp64(ad, bd, c.data(), h, w, wB, d, scratch(need), need, nullptr),
           "dense product");
   } else {
+    int moduli = 0;
+    const size_t qneed = (size_t)h * 16 + 768;
+    check(lnt_dense_crt_moduli(ad, bd, h, w, wB, d, 1e-12, scratch(qneed), qneed, &moduli, nullptr),
+          "dense product");
     size_t need = 0;
-    check(lnt_dense_split_workspace(h, w, wB, s, &need), "dense product");
-    check(lnt_dense_lattice_mult_split(ad, bd, c.data(), h, w, wB, d, s, scratch(need), need, nullptr),
+    check(lnt_dense_crt_workspace(h, w, wB, moduli, &need), "dense product");
+    check(lnt_dense_lattice_mult_crt(ad, bd, c.data(), h, w, wB, d, moduli, scratch(need), need, nullptr),
           "dense product");
   }
   return {std::move(c), std::move(labels), o.l_inter.size()};

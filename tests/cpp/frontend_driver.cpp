@@ -217,7 +217,9 @@ int main(int argc, char** argv) {
       lnt::DenseNT<4> a(d2, d1, d2, d1), b(d1, d2, d1, d2), c(d1, d1, d1, d1);
       a.upload(read_raw<double>(g_dir + "/A.vals"));
       b.upload(read_raw<double>(g_dir + "/B.vals"));
-      lnt::DenseTensor::slices() = slices;
+      lnt::DenseTensor::slices() = slices > 0 ? slices : 0;
+      lnt::DenseTensor::precision() =
+          slices < 0 ? lnt::DenseTensor::Precision::Float64 : lnt::DenseTensor::Precision::Emulated;
       c(i, j, m, n) = a(k, i, l, j) * b(m, k, n, l);
       std::vector<double> h;
       c.download(h);
@@ -264,7 +266,9 @@ int main(int argc, char** argv) {
       lnt::DenseNT<4> a(d1, d1, d2, d2), b(d2, d2, d1, d1), c(d1, d1, d1, d1);
       a.upload(read_raw<double>(g_dir + "/A.vals"));
       b.upload(read_raw<double>(g_dir + "/B.vals"));
-      lnt::DenseTensor::slices() = slices;
+      lnt::DenseTensor::slices() = slices > 0 ? slices : 0;
+      lnt::DenseTensor::precision() =
+          slices < 0 ? lnt::DenseTensor::Precision::Float64 : lnt::DenseTensor::Precision::Emulated;
       c(i, j, m, n) = a(i, j, k, l) * b(k, l, m, n);
       std::vector<double> h;
       c.download(h);

@@ -94,6 +94,43 @@ def test_crt_golden_fixture_and_kat(cuda, torch):
     assert np.all(c == ww * (ww + 1) / 2)
 
 
+@pytest.mark.parametrize("h,w,wB", [(600, 2000, 700), (256, 256, 256), (1, 130, 513), (300, 64, 3),
+                                    (513, 4100, 257)])
+@pytest.mark.parametrize("moduli", [13, 16])
+def test_crt_integer_operands_exact(cuda, torch, rng, h, w, wB, moduli):
+    """Integer operands (|a|, |b| <= 1000) are scaled by powers of two into
+    integers without rounding, so scheme II must return A B exactly: every
+    residue product tile of the tensor-core GEMM (partial row, column and K
+    tiles included) is checked bit for bit."""
+    A = rng.integers(-1000, 1001, h * w).astype(np.float64)
+    B = rng.integers(-1000, 1001, w * wB).astype(np.float64)
+    C = to_host(cuda.dense_mult_crt(to_dev(A, torch), to_dev(B, torch), h, w, wB, 1, moduli=moduli))
+    ref = (A.reshape(w, h).T @ B.reshape(wB, w).T).T.ravel()  # column-major C, exact in float64
+    np.testing.assert_array_equal(C, ref)
+
+
+@pytest.mark.parametrize("variant,w,expect", [("uniform", 16384, 14), ("uniform", 4096, 13),
+                                              ("wide_exponent", 16384, 15)])
+def test_crt_moduli_choice_meets_tolerance(cuda, torch, rng, variant, w, expect):
+    """lnt_dense_crt_moduli: the smallest count whose bound 2^(2-beta) R keeps
+    every entry within 1e-12 of |A||B|, R the largest max / mean magnitude
+    ratio of a row of A or column of B; the product with that count meets it."""
+    h, wB = 48, 40
+    if variant == "uniform":
+        A, B = rng.uniform(-1, 1, h * w), rng.uniform(-1, 1, w * wB)
+    else:
+        A = rng.uniform(1, 2, h * w) * 2.0 ** rng.integers(-20, 21, h * w) * rng.choice([-1, 1], h * w)
+        B = rng.uniform(1, 2, w * wB) * 2.0 ** rng.integers(-20, 21, w * wB) * rng.choice([-1, 1], w * wB)
+    Ad, Bd = to_dev(A, torch), to_dev(B, torch)
+    m = cuda.dense_crt_moduli(Ad, Bd, h, w, wB)
+    assert m == expect
+    Cs = to_host(cuda.dense_mult_crt(Ad, Bd, h, w, wB, 1, moduli=m))
+    rows, cols = np.meshgrid(np.arange(h), np.arange(wB), indexing="ij")
+    ref, mag = oracle.dense_entries(A, B, h, w, rows.ravel(), cols.ravel())
+    got = Cs.reshape(wB, h).T.ravel()
+    assert np.max(np.abs(got - ref) / mag) <= 1e-12
+
+
 @pytest.mark.parametrize("h,w,wB,d", [(100, 300, 70, 3), (257, 1000, 129, 1), (64, 4096, 64, 1)])
 @pytest.mark.parametrize("variant", ["uniform", "wide_exponent"])
 @pytest.mark.parametrize("moduli", [13, 16])

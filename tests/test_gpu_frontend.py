@@ -195,9 +195,10 @@ def test_sort_seq_and_collect(driver, tmp_path, rng, n, sorted_):
     same(read(tmp_path, "c"), e2)
 
 
-@pytest.mark.parametrize("slices", [0, 7])
+@pytest.mark.parametrize("slices", [-1, 0, 7])
 def test_dense_product(driver, tmp_path, rng, slices):
-    """c(i,j,m,n) = a(i,j,k,l) * b(k,l,m,n) on DenseNT<4>, float64 and split."""
+    """c(i,j,m,n) = a(i,j,k,l) * b(k,l,m,n) on DenseNT<4>: plain float64 (-1),
+    the default emulated scheme II (0) and scheme I slices (7)."""
     d1, d2 = 6, 5
     A = rng.uniform(-1, 1, d1 * d1 * d2 * d2)
     B = rng.uniform(-1, 1, d2 * d2 * d1 * d1)
@@ -237,7 +238,7 @@ def colmajor_permute(x, dims, perm):
     return np.ravel(np.asarray(x).reshape(dims, order="F").transpose(perm), order="F")
 
 
-@pytest.mark.parametrize("slices", [0, 7])
+@pytest.mark.parametrize("slices", [-1, 0, 7])
 def test_dense_product_permuted_operands(driver, tmp_path, rng, slices):
     """c(i,j,m,n) = a(k,i,l,j) * b(m,k,n,l): neither operand in lattice order,
     so both go through a permuted copy (latticeCopy) first."""
