@@ -325,8 +325,8 @@ LNT_API int lnt_contract_attract(const uint64_t* keys, const double* vals, size_
 
 /* ---- batched lattice products ------------------------------------------- */
 
-/* `count` independent products C_p = A_p * B_p, each as lnt_lattice_mult,
- * with at most 1024 rows per A_p.  Host arrays: dims_host[4p..4p+3] =
+/* `count` independent products C_p = A_p * B_p, each as lnt_lattice_mult
+ * (rows beyond 1024 are accumulated in blocks of 1024).  Host arrays: dims_host[4p..4p+3] =
  * (rows(A_p), cols(A_p) = rows(B_p), cols(B_p), tabs); a_off_host / b_off_host
  * (count+1 entries) delimit each problem's operand inside the concatenated
  * device arrays a_keys/a_vals, b_keys/b_vals (each lattice key-sorted).
@@ -348,6 +348,32 @@ LNT_API int lnt_batched_lattice_mult(int count, const int64_t* dims_host, const 
                                      const double* a_vals, const uint64_t* b_keys, const double* b_vals,
                                      void* workspace, size_t workspace_bytes, uint64_t* c_keys,
                                      double* c_vals, uint64_t* d_c_off, void* stream);
+
+/* The same batch with the operands as the tensors store them: unsorted, each
+ * key linearised in its tensor's own mode order.  Problem p's A keys are
+ * re-keyed by a_rekey_host[p] and its B keys by b_rekey_host[p] into lattice
+ * order (order 0 = already in lattice order; NULL array = all order 0), and
+ * both are sorted inside the call -- the per-product toLatticeSort of the
+ * reference (SparseMIABase.h:1457-1586; for c(i,l) = a(i,j,k) * b(k,l,j): A
+ * as it is, B to the mode order {2,0,1}, SparseMIABase.h:1527-1586) done for
+ * the whole batch by one radix sort over keys prefixed with the problem index
+ * -- then multiplied as lnt_batched_lattice_mult does.  Keys must lie below
+ * their lattice's size (rows x cols x tabs).  a_off_host[0] and b_off_host[0]
+ * must be 0, and the batch holds fewer than 2^30 pairs.  Call
+ * lnt_batched_contract_prepare once per batch layout (synchronous uploads),
+ * then lnt_batched_contract, which only enqueues work on `stream` and can be
+ * captured into a CUDA graph. */
+LNT_API int lnt_batched_contract_workspace(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                                           const uint64_t* b_off_host, size_t* bytes, uint64_t* c_capacity);
+LNT_API int lnt_batched_contract_prepare(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                                         const uint64_t* b_off_host, const lnt_rekey_spec* a_rekey_host,
+                                         const lnt_rekey_spec* b_rekey_host, void* workspace,
+                                         size_t workspace_bytes, void* stream);
+LNT_API int lnt_batched_contract(int count, const int64_t* dims_host, const uint64_t* a_off_host,
+                                 const uint64_t* b_off_host, const uint64_t* a_keys, const double* a_vals,
+                                 const uint64_t* b_keys, const double* b_vals, void* workspace,
+                                 size_t workspace_bytes, uint64_t* c_keys, double* c_vals, uint64_t* d_c_off,
+                                 void* stream);
 
 /* ---- dense lattice product ---------------------------------------------- */
 

@@ -117,6 +117,10 @@ _SIGS = {
     "lnt_batched_workspace": ([C.c_int, _vp, _vp, _vp, C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)], C.c_int),
     "lnt_batched_prepare": ([C.c_int, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
     "lnt_batched_lattice_mult": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp], C.c_int),
+    "lnt_batched_contract_workspace": ([C.c_int, _vp, _vp, _vp, C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)],
+                                       C.c_int),
+    "lnt_batched_contract_prepare": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp], C.c_int),
+    "lnt_batched_contract": ([C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp], C.c_int),
     "lnt_dense_fp64_workspace": ([C.POINTER(C.c_size_t)], C.c_int),
     "lnt_dense_lattice_mult_fp64": ([_vp, _vp, _vp, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _vp, _sz, _vp],
                                     C.c_int),
@@ -468,36 +472,59 @@ class Batch:
     """A batch of lattice products on one device (see lnt_batched_* in include/lnt.h).
 
     dims: int64 array (count, 4) of (h, w, wB, d); a_off / b_off: uint64 (count+1)
-    offsets into the concatenated device tensors a_keys/a_vals, b_keys/b_vals."""
+    offsets into the concatenated device tensors a_keys/a_vals, b_keys/b_vals.
+    Without re-key specs the operands are key-sorted lattices
+    (lnt_batched_lattice_mult); with a_rekey / b_rekey (a sequence of count
+    RekeySpec, or None for "already in lattice order") they are unsorted tensors
+    that the call re-keys and sorts (lnt_batched_contract)."""
 
-    def __init__(self, dims, a_off, b_off, a_keys, a_vals, b_keys, b_vals):
+    def __init__(self, dims, a_off, b_off, a_keys, a_vals, b_keys, b_vals, a_rekey=None, b_rekey=None):
         torch = _torch()
         self.count = int(len(dims))
         self.dims = np.ascontiguousarray(dims, np.int64)
         self.a_off = np.ascontiguousarray(a_off, np.uint64)
         self.b_off = np.ascontiguousarray(b_off, np.uint64)
         self.tensors = (a_keys, a_vals, b_keys, b_vals)
+        self.contract = a_rekey is not None or b_rekey is not None
+        pre = "lnt_batched_contract" if self.contract else "lnt_batched"
         dev = a_keys.device
         nb = C.c_size_t(0)
         cap = C.c_uint64(0)
-        _check(lib().lnt_batched_workspace(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
-                                           self.b_off.ctypes.data, C.byref(nb), C.byref(cap)), "lnt_batched_workspace")
+        _check(getattr(lib(), pre + "_workspace")(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
+                                                  self.b_off.ctypes.data, C.byref(nb), C.byref(cap)),
+               pre + "_workspace")
         self.ws = workspace(nb.value, dev)
         self.capacity = int(cap.value)
         self.c_keys = torch.empty(max(self.capacity, 1), dtype=torch.int64, device=dev)
         self.c_vals = torch.empty(max(self.capacity, 1), dtype=torch.float64, device=dev)
         self.c_off = torch.zeros(self.count + 1, dtype=torch.int64, device=dev)
-        _check(lib().lnt_batched_prepare(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
-                                         self.b_off.ctypes.data, _ptr(self.ws), self.ws.numel(), _stream()),
-               "lnt_batched_prepare")
+        if self.contract:
+            specs = []
+            for seq in (a_rekey, b_rekey):
+                arr = (RekeySpec * self.count)()
+                if seq is not None:
+                    for p, sp in enumerate(seq):
+                        if sp is not None:
+                            arr[p] = sp
+                specs.append(arr)
+            self._specs = specs
+            _check(lib().lnt_batched_contract_prepare(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
+                                                      self.b_off.ctypes.data, C.cast(specs[0], _vp),
+                                                      C.cast(specs[1], _vp), _ptr(self.ws), self.ws.numel(),
+                                                      _stream()), "lnt_batched_contract_prepare")
+        else:
+            _check(lib().lnt_batched_prepare(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
+                                             self.b_off.ctypes.data, _ptr(self.ws), self.ws.numel(), _stream()),
+                   "lnt_batched_prepare")
 
     def run(self):
         """Enqueue the batched product on the current stream (capturable)."""
         ak, av, bk, bv = self.tensors
-        _check(lib().lnt_batched_lattice_mult(self.count, self.dims.ctypes.data, self.a_off.ctypes.data,
-                                              self.b_off.ctypes.data, _ptr(ak), _ptr(av), _ptr(bk), _ptr(bv),
-                                              _ptr(self.ws), self.ws.numel(), _ptr(self.c_keys), _ptr(self.c_vals),
-                                              _ptr(self.c_off), _stream()), "lnt_batched_lattice_mult")
+        f = lib().lnt_batched_contract if self.contract else lib().lnt_batched_lattice_mult
+        _check(f(self.count, self.dims.ctypes.data, self.a_off.ctypes.data, self.b_off.ctypes.data, _ptr(ak),
+                 _ptr(av), _ptr(bk), _ptr(bv), _ptr(self.ws), self.ws.numel(), _ptr(self.c_keys),
+                 _ptr(self.c_vals), _ptr(self.c_off), _stream()),
+               "lnt_batched_contract" if self.contract else "lnt_batched_lattice_mult")
 
     def result(self, p):
         off = self.c_off.tolist()

@@ -81,13 +81,126 @@ def test_batched_cuda_graph_replay(cuda, torch, rng):
     check_batch(cuda, torch, batch, dims, ak, av, bk, bv)
 
 
-def test_batched_rejects_tall_problems(cuda, torch):
-    import ctypes as C
-
+def test_batched_rows_beyond_one_accumulator(cuda, torch, rng):
+    """Problems with more than 1024 rows are accumulated in blocks of 1024 rows
+    (a binary search per A column and block): same results as the oracle."""
     import libnt_b200 as L
-    dims = np.array([[2048, 4, 4, 1]], np.int64)  # beyond the 1024-row accumulator
-    off = np.array([0, 0], np.uint64)
-    nb, cap = C.c_size_t(0), C.c_uint64(0)
-    st = L.lib().lnt_batched_workspace(1, dims.ctypes.data, off.ctypes.data, off.ctypes.data, C.byref(nb),
-                                       C.byref(cap))
-    assert st == 8  # LNT_UNSUPPORTED
+    dims, ak, av, bk, bv = [], [], [], [], []
+    for h, w, wB, na, nb in [(3000, 40, 30, 20000, 500), (1025, 8, 9, 4000, 50), (2048, 1, 3, 2048, 3),
+                             (5000, 16, 4, 0, 30), (1500, 20, 20, 6000, 0)]:
+        a = np.sort(rng.choice(h * w, na, replace=False)).astype(np.uint64)
+        b = np.sort(rng.choice(w * wB, nb, replace=False)).astype(np.uint64)
+        dims.append((h, w, wB, 1))
+        ak.append(a)
+        bk.append(b)
+        av.append(rng.uniform(-1, 1, na))
+        bv.append(rng.uniform(-1, 1, nb))
+    a_off = np.concatenate([[0], np.cumsum([x.size for x in ak])]).astype(np.uint64)
+    b_off = np.concatenate([[0], np.cumsum([x.size for x in bk])]).astype(np.uint64)
+    dims = np.array(dims, np.int64)
+    batch = L.Batch(dims, a_off, b_off, to_dev(np.concatenate(ak), torch), to_dev(np.concatenate(av), torch),
+                    to_dev(np.concatenate(bk), torch), to_dev(np.concatenate(bv), torch))
+    batch.run()
+    check_batch(cuda, torch, batch, dims, ak, av, bk, bv)
+    assert cuda.device_status() == 0
+
+
+def _unsorted_batch(rng, count, dim_lo, dim_hi, nnz_lo, nnz_hi, tall=()):
+    """Problems c(i,l) = a(j,i,k) * b(k,l,j) as unsorted tensors: a's keys run j
+    fastest (re-key {1,0,2} puts i first), b's keys k fastest (re-key {2,0,1});
+    `tall` problems get i beyond the 1024-row accumulator."""
+    import libnt_b200 as L
+    dims, specs_a, specs_b, ak, av, bk, bv = [], [], [], [], [], [], []
+    for p in range(count):
+        i, j, k, l = (int(x) for x in rng.integers(dim_lo, dim_hi + 1, 4))
+        if p in tall:
+            i = 1500 + 37 * p
+        na = min(int(round(10 ** rng.uniform(np.log10(nnz_lo), np.log10(nnz_hi)))), i * j * k)
+        nb = min(int(round(10 ** rng.uniform(np.log10(nnz_lo), np.log10(nnz_hi)))), k * l * j)
+        if p % 17 == 5:
+            na = 0  # empty operands
+        if p % 19 == 7:
+            nb = 0
+        ak.append(rng.permutation(rng.choice(j * i * k, na, replace=False)).astype(np.uint64))
+        bk.append(rng.permutation(rng.choice(k * l * j, nb, replace=False)).astype(np.uint64))
+        av.append(rng.uniform(-1, 1, na))
+        bv.append(rng.uniform(-1, 1, nb))
+        dims.append((i, j * k, l, 1))
+        specs_a.append(((j, i, k), [0, 1, 2], [1, 0, 2]))
+        specs_b.append(((k, l, j), [0, 1, 2], [2, 0, 1]))
+    a_off = np.concatenate([[0], np.cumsum([x.size for x in ak])]).astype(np.uint64)
+    b_off = np.concatenate([[0], np.cumsum([x.size for x in bk])]).astype(np.uint64)
+    ra = [L.RekeySpec.make(*x) for x in specs_a]
+    rb = [L.RekeySpec.make(*x) for x in specs_b]
+    return np.array(dims, np.int64), a_off, b_off, ak, av, bk, bv, specs_a, specs_b, ra, rb
+
+
+def _expected_unsorted(p, dims, ak, av, bk, bv, specs_a, specs_b):
+    h, w, wB, _ = (int(x) for x in dims[p])
+    ka = oracle.rekey(ak[p], *specs_a[p])
+    kb = oracle.rekey(bk[p], *specs_b[p])
+    oa, ob = np.argsort(ka, kind="stable"), np.argsort(kb, kind="stable")
+    return oracle.lattice_mult(ka[oa], av[p][oa], h, w, 1, kb[ob], bv[p][ob], wB, with_abs=True)
+
+
+def test_batched_contract_unsorted_matches_oracle(cuda, torch, rng):
+    """lnt_batched_contract on unsorted tensors: every problem re-keyed into its
+    lattice order and sorted inside the call (one radix sort over keys prefixed
+    with the problem), then multiplied; replayed from a CUDA graph on new
+    values.  Each problem equals re-key + sort + csc_no_accum on the host."""
+    import libnt_b200 as L
+    dims, a_off, b_off, ak, av, bk, bv, sa, sb, ra, rb = _unsorted_batch(rng, 150, 4, 60, 3, 4000, tall=(3, 77))
+    dk = [to_dev(np.concatenate(x), torch) for x in (ak, av, bk, bv)]
+    batch = L.Batch(dims, a_off, b_off, *dk, a_rekey=ra, b_rekey=rb)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        batch.run()
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    for p in range(len(dims)):
+        ek, ev, ea = _expected_unsorted(p, dims, ak, av, bk, bv, sa, sb)
+        k, v = batch.result(p)
+        np.testing.assert_array_equal(to_host(k, np.uint64), ek)
+        assert rel_ok(to_host(v), ev, ea)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        batch.run()
+    av = [rng.uniform(-1, 1, x.size) for x in av]
+    dk[1].copy_(to_dev(np.concatenate(av), torch))
+    batch.c_vals.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    for p in range(len(dims)):
+        ek, ev, ea = _expected_unsorted(p, dims, ak, av, bk, bv, sa, sb)
+        k, v = batch.result(p)
+        np.testing.assert_array_equal(to_host(k, np.uint64), ek)
+        assert rel_ok(to_host(v), ev, ea)
+    assert cuda.device_status() == 0
+    del g
+
+
+def test_batched_contract_full_workload(cuda, torch):
+    """The benchmarked batch: 4096 problems c(i,l) = a(i,j,k) * b(k,l,j), dims
+    U{16..512}, nnz log-U[1e2, 1e5], both operands unsorted; every problem
+    checked against the oracle (keys exact, values within 1e-12 of the sum of
+    |products| per key)."""
+    import bench
+    import libnt_b200 as L
+    dims, tdims, a_off, b_off, ak, av, bk, bv = bench.batched_inputs()
+    count = len(dims)
+    dk = [to_dev(np.concatenate(x), torch) for x in (ak, av, bk, bv)]
+    rb = [L.RekeySpec.make(tdims[p][1], [0, 1, 2], [2, 0, 1]) for p in range(count)]
+    batch = L.Batch(dims, a_off, b_off, *dk, a_rekey=[None] * count, b_rekey=rb)
+    batch.run()
+    torch.cuda.synchronize()
+    assert cuda.device_status() == 0
+    off = batch.c_off.cpu().numpy()
+    ck = batch.c_keys[: int(off[-1])].cpu().numpy().view(np.uint64)
+    cv = batch.c_vals[: int(off[-1])].cpu().numpy()
+    del dk, batch
+    torch.cuda.empty_cache()
+    for p in range(count):
+        ek, ev, ea = bench.batched_expected(p, dims, tdims, ak, av, bk, bv, with_abs=True)
+        np.testing.assert_array_equal(ck[off[p]:off[p + 1]], ek)
+        assert rel_ok(cv[off[p]:off[p + 1]], ev, ea), p
