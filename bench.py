@@ -145,8 +145,9 @@ def dist_setup(n_gpus: int):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if not dist.is_initialized():
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return world, rank, local
@@ -415,7 +416,8 @@ def run_ours(args):
     value = job_throughput(n, world, ms)
     os_ms, os_launches = L.profile_query("sort_onesweep")
     kernels = {}
-    for name in ("sort_hist", "sort_onesweep", "bucket_sort_collect", "collect_lead", "collect"):
+    for name in ("sort_hist", "sort_onesweep", "bucket_sort_collect", "collect_lead", "collect",
+                 "sort_hist_fallback", "sort_onesweep_fallback", "collect_lead_fallback", "collect_fallback"):
         t, c = L.profile_query(name)
         kernels[name] = {"ms_total": t, "launches": c}
     L.profile_reset()
@@ -502,6 +504,19 @@ def run_ours(args):
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "traffic": (tpp * n) if tpp else None}
     step_alg = 16.0 * n + 16.0 * n_out
+    extra = {}
+    if world == 1 and not args.no_extra:
+        # the metric's other two parts, measured in the same run: the skewed
+        # contraction (products/s) and the emulated FP64 dense contraction
+        del ak, av, bk, bv, out_k, out_v, ws
+        torch.cuda.empty_cache()
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup, sub.no_scheme1 = min(args.steps, 5), 3, True
+        for key, fn in (("skewed_contraction", measure_skewed), ("dense", measure_dense)):
+            d = fn(sub)
+            torch.cuda.empty_cache()
+            if d is not None:
+                extra[key] = {k: v for k, v in d.items() if k not in ("metric", "n_gpus", "scaling", "vs_baseline", "data")}
     result = None
     if rank == 0:
         cpu = None
@@ -529,6 +544,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": sampler.summary(),
         }
+        result.update(extra)
         print(json.dumps(result), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -887,9 +903,17 @@ def run_batched(args):
 
 
 def run_dense(args):
+    d = measure_dense(args)
+    if d is not None:
+        print(json.dumps(d), flush=True)
+    return 0
+
+
+def measure_dense(args):
     """c(i,j,m,n) = a(i,j,k,l) * b(k,l,m,n), all dims 128: a 16384^3 FP64 GEMM.
     Headline: scheme II (moduli + Chinese remaindering) on INT8 tensor cores;
-    also timed: scheme I (INT8 slices) and the plain FP64 GEMM."""
+    also timed: scheme I (INT8 slices) and the plain FP64 GEMM.  Returns the
+    JSON line (rank 0) or None."""
     import torch
 
     import libnt_b200 as L
@@ -977,7 +1001,7 @@ def run_dense(args):
         del A, B, Cc, C64
         torch.cuda.empty_cache()
     if rank != 0:
-        return 0
+        return None
     # INT8 tensor peak measured here (torch._int_mm 8192^3), the roofline denominator
     a8 = torch.randint(-64, 64, (8192, 8192), device=dev, dtype=torch.int8)
     b8 = torch.randint(-64, 64, (8192, 8192), device=dev, dtype=torch.int8)
@@ -997,15 +1021,14 @@ def run_dense(args):
                           "<= 256 as INT8 tensor-core GEMMs (this library's tcgen05 kernel, products reduced "
                           "modulo m in its epilogue), Chinese remaindering in exact integer limbs",
               "variants": results}
-    print(json.dumps(_line("TFLOP/s (FP64-equivalent)", u["effective_fp64_tflops"], u["crt_ms"], args, world,
-                           config, {
+    return _line("TFLOP/s (FP64-equivalent)", u["effective_fp64_tflops"], u["crt_ms"], args, world,
+                 config, {
         "roofline": {"bound": "tensor", "kernel": "mod_gemm_kernel (tcgen05 INT8 products of all moduli, "
                                                   "reduced modulo m in the epilogue)", "achieved": u["int8_tensor_tops"],
                      "peak": int8_peak, "unit": "TOP/s", "frac": u["int8_tensor_tops"] / int8_peak,
                      "peak_source": "int8 torch._int_mm 8192^3 measured in this run (MEASURED_PEAKS.json has bf16 only)"},
         "vs_fp64_gemm": u["speedup_vs_fp64"], "clocks": u["clocks"],
-    })), flush=True)
-    return 0
+    })
 
 def _timed_steps(torch, step, args):
     """W untimed steps, then K timed steps with CUDA events on the current
@@ -1383,9 +1406,17 @@ def skewed_inputs_cpu(nnz_a, nnz_b, dims=SKEW_DIMS, seed=0):
 
 
 def run_skewed(args):
+    d = measure_skewed(args)
+    if d is not None:
+        print(json.dumps(d), flush=True)
+    return 0
+
+
+def measure_skewed(args):
     """Large skewed sparse contraction c(i,j,m) = a(i,j,k,l) * b(k,l,m) on
     key-sorted lattices; a step = lnt_lattice_mult_plan (product count) +
-    lnt_lattice_mult (the tile engine at this shape) through the C ABI."""
+    lnt_lattice_mult (the tile engine at this shape) through the C ABI.
+    Returns the JSON line (rank 0) or None."""
     import ctypes as C
 
     import torch
@@ -1470,7 +1501,7 @@ def run_skewed(args):
              "tile_cbits", "tile_count", "tile_scan", "tile_numeric")
     kernels = {k: L.profile_query(k)[0] / args.steps for k in names}
     if rank != 0:
-        return 0
+        return None
     peak, peak_kind = peaks()
     alg = 16.0 * (ak.numel() + bk.numel() + n_out)
     num_ms = kernels["tile_numeric"]
@@ -1496,7 +1527,7 @@ def run_skewed(args):
                           "product on key-sorted lattices",
               "nnz_a": int(ak.numel()), "nnz_b": int(bk.numel()), "products": products, "output_nnz": n_out,
               "l2": "output (16 B x output nnz) far larger than L2", "parallelism": "1 GPU"}
-    print(json.dumps(_line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
+    return _line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
         "gpu_launches": launches, "kernels_ms_per_step": kernels, "spot_check_max_rel_err": spot,
         "roofline": {"bound": "hbm", "kernel": "tile_numeric (products, staging, output write)",
                      "achieved": alg / (num_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -1506,8 +1537,7 @@ def run_skewed(args):
                      "traffic": (tpo * n_out) if tpo else None,
                      "traffic_note": "DRAM bytes per output entry from the small-case ncu capture, times the output count"},
         "cpu_baseline": cpu, "clocks": sampler.summary(),
-    })), flush=True)
-    return 0
+    })
 
 
 def main():
@@ -1520,6 +1550,8 @@ def main():
     ap.add_argument("--nnz-log2", type=int, default=26,
                     help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="merge line only: skip the skewed-contraction and dense keys")
     ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed", "outer", "unary", "scanmerge", "mixed"],
                     help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
                          "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")

@@ -375,13 +375,13 @@ int run_collect_gated(const u64* keys, const double* vals, size_t n, int skip_ze
   LeadSummary* lead = reinterpret_cast<LeadSummary*>(w + L.off_lead);
   const u32 lead_blocks = (L.ntiles + 3) / 4;
   {
-    ProfScope prof("collect_lead", s);
+    ProfScope prof(gate ? "collect_lead_fallback" : "collect_lead", s);
     lead_kernel<<<gate ? std::min(lead_blocks, (u32)sm_count() * 8u) : lead_blocks, 128, 0, s>>>(
         keys, vals, n, L.ntiles, lead, gate, want);
   }
   unsigned long long* status = reinterpret_cast<unsigned long long*>(w + L.off_status);
   u32* counter = reinterpret_cast<u32*>(w + L.off_counter);
-  ProfScope prof("collect", s);
+  ProfScope prof(gate ? "collect_fallback" : "collect", s);
   if (gate) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, collect_kernel<true>, kThreads, 0) != cudaSuccess)

@@ -451,7 +451,7 @@ int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, d
     if (sh > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     const int blocks =
         std::max(1, std::min((int)((plan.n + kThreads * 16 - 1) / (kThreads * 16)), sm_count() * 4));
-    ProfScope prof("sort_hist", s);
+    ProfScope prof(src.gate ? "sort_hist_fallback" : "sort_hist", s);
     kern<<<blocks, kThreads, sh, s>>>(src, plan.n, plan.passes, plan.key_bits, ghist, bstart,
                                       counters + plan.passes);
     count_launch();
@@ -484,7 +484,7 @@ int run_sort_variant(const SortPlan& plan, const PairSource& src, u64* buf0_k, d
     const int w = std::min(BITS, plan.key_bits - shift);
     const u32 mask = (1u << w) - 1u;
     u32* st = status + (size_t)p * plan.ntiles * RADIX;
-    ProfScope prof("sort_onesweep", s);
+    ProfScope prof(gated ? "sort_onesweep_fallback" : "sort_onesweep", s);
     if (p == 0) {
       if (gated)
         onesweep_kernel<BITS, THREADS, ITEMS, W, true, true><<<grid, THREADS, sh, s>>>(
