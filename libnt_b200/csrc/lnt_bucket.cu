@@ -25,16 +25,30 @@
 #include <cstdlib>
 
 #include "lnt_sort.cuh"
+#include "lnt_tuned.h"
 
 namespace lnt {
 namespace {
 
 constexpr int kHistThreads = 1024;
-constexpr int kBT = 512;                 // bucket CTA threads
-constexpr int kBWarps = kBT / 32;
-constexpr int kBItems = 10;
-constexpr int kBCap = kBT * kBItems;     // 5120 pairs per bucket
-constexpr int kIdxBits = 13;             // local index field (kBCap <= 8192)
+// Bucket geometries (the bucket kernel's CTA size, pairs per thread, bits of
+// the local index field and of the counting pass).  Large: 2^(lg n - 12)
+// buckets of about 4096 pairs (at most 5120), 512-thread CTAs.  Small:
+// 2^(lg n - 11) buckets of about 2048 pairs (at most 2560), 256-thread CTAs,
+// more of them resident per SM.
+template <int BT, int ITEMS, int IDXB, int SUBB>
+struct BucketGeom {
+  static constexpr int kBT = BT;
+  static constexpr int kBWarps = BT / 32;
+  static constexpr int kBItems = ITEMS;
+  static constexpr int kBCap = BT * ITEMS;
+  static constexpr int kIdxBits = IDXB;  // kBCap <= 2^IDXB
+  static constexpr int kSubBits = SUBB;
+  static constexpr int kSlots = kBCap + kBCap / 32;
+  static constexpr int kMinBlocks = BT >= 512 ? 2 : 4;
+};
+using GeomLarge = BucketGeom<512, 10, 13, 12>;
+using GeomSmall = BucketGeom<256, 10, 12, 11>;
 constexpr int kLBits = 7;                // bits per local pass
 constexpr int kLRadix = 1 << kLBits;
 constexpr unsigned long long kFlagAgg = 1ull << 62;
@@ -47,6 +61,8 @@ struct BucketCtrl {
   u32* start;        // 2^T + 1
   u32* bstart_a;     // 256
   u32* bstart_b;     // 256
+  u32* digits_a;     // 256: pass A digit counts
+  u32* digits_b;     // 256: pass B digit counts
   u32* misc;         // [0] max bucket, [1] hist done, [2] pass A tiles, [3] pass B tiles, [4] bucket counter
   u32* status_a;     // ntiles x 256
   u32* status_b;     // ntiles x 256
@@ -54,13 +70,34 @@ struct BucketCtrl {
   u32* gate;         // written by the histogram: 0 = every bucket fits a CTA, 1 = take the LSD path
 };
 
-__global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const PairSource src, u32 n, int T, int low_bits,
-                                                                   BucketCtrl c) {
-  extern __shared__ u32 sh[];  // 2^T
-  const int nb = 1 << T;
-  for (int i = threadIdx.x; i < nb; i += kHistThreads) sh[i] = 0;
+// Bucket counts in shared memory as 16-bit fields (two per word, 2^T / 2
+// words: 64 KB at T = 15, so two 1024-thread CTAs fit per SM).  A field keeps
+// 15 bits; the increment that takes it to 2^15 moves 2^15 to the bucket's
+// global count and clears bit 15 again, so no field carries into its
+// neighbour (the other increments that can land in between are far fewer
+// than 2^15).
+__device__ __forceinline__ void count16(u32* sh, u32 b, const BucketCtrl& c, int TA) {
+  const u32 sh_bits = 16u * (b & 1u);
+  const u32 old = atomicAdd(&sh[b >> 1], 1u << sh_bits);
+  if (((old >> sh_bits) & 0x7FFFu) == 0x7FFFu) {  // rare: once per 2^15 keys of one bucket in one CTA
+    atomicSub(&sh[b >> 1], 0x8000u << sh_bits);
+    atomicAdd(&c.counts[b], 0x8000u);
+    atomicAdd(&c.digits_a[b & ((1u << TA) - 1u)], 0x8000u);
+    atomicAdd(&c.digits_b[b >> TA], 0x8000u);
+  }
+}
+
+__global__ void __launch_bounds__(kHistThreads, 2) bucket_hist_kernel(const PairSource src, u32 n, int T, int low_bits,
+                                                                   u32 cap, BucketCtrl c) {
+  extern __shared__ u32 sh[];  // 2^T 16-bit fields
+  __shared__ u32 s_ha[256], s_hb[256];
+  const int nb = 1 << T, nw = nb >> 1;
+  const int TA = T - 8;
+  for (int i = threadIdx.x; i < nw; i += kHistThreads) sh[i] = 0;
+  if (threadIdx.x < 256) s_ha[threadIdx.x] = s_hb[threadIdx.x] = 0;
   __syncthreads();
   const u32 stride = gridDim.x * kHistThreads;
+  const u32 bmask = (u32)(nb - 1);
   constexpr int U = 8;
   u32 i = blockIdx.x * kHistThreads + threadIdx.x;
   for (; i + (U - 1) * stride < n; i += U * stride) {
@@ -71,15 +108,28 @@ __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const PairSou
       k[u] = x < src.na ? rekey(__ldcs(src.ak + x), src.ra) : rekey(__ldcs(src.bk + (x - src.na)), src.rb);
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) atomicAdd(&sh[(u32)(k[u] >> low_bits) & (u32)(nb - 1)], 1u);
+    for (int u = 0; u < U; ++u) count16(sh, (u32)(k[u] >> low_bits) & bmask, c, TA);
   }
   for (; i < n; i += stride) {
     const u64 k = i < src.na ? rekey(__ldcs(src.ak + i), src.ra) : rekey(__ldcs(src.bk + (i - src.na)), src.rb);
-    atomicAdd(&sh[(u32)(k >> low_bits) & (u32)(nb - 1)], 1u);
+    count16(sh, (u32)(k >> low_bits) & bmask, c, TA);
   }
   __syncthreads();
-  for (int b = threadIdx.x; b < nb; b += kHistThreads)
-    if (sh[b]) atomicAdd(&c.counts[b], sh[b]);
+  // flush: bucket counts, and this CTA's share of the two passes' digit counts
+  // (pass A digit = bucket & (2^TA - 1), pass B digit = bucket >> TA)
+  for (int b = threadIdx.x; b < nb; b += kHistThreads) {
+    const u32 v = (sh[b >> 1] >> (16 * (b & 1))) & 0xFFFFu;
+    if (v) {
+      atomicAdd(&c.counts[b], v);
+      atomicAdd(&s_ha[b & ((1 << TA) - 1)], v);
+      atomicAdd(&s_hb[b >> TA], v);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 256) {
+    if (s_ha[threadIdx.x]) atomicAdd(&c.digits_a[threadIdx.x], s_ha[threadIdx.x]);
+    if (s_hb[threadIdx.x]) atomicAdd(&c.digits_b[threadIdx.x], s_hb[threadIdx.x]);
+  }
   __threadfence();
   __syncthreads();
   __shared__ bool s_last;
@@ -95,7 +145,6 @@ __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const PairSou
   for (int j = 0; j < per; ++j) {
     const int b = tid * per + j;
     const u32 v = b < nb ? __ldcg(&c.counts[b]) : 0u;
-    if (b < nb) sh[b] = v;  // this CTA's own counts were flushed above
     local += v;
     mx = max(mx, v);
   }
@@ -113,7 +162,7 @@ __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const PairSou
     const int b = tid * per + j;
     if (b < nb) {
       c.start[b] = run;
-      run += sh[b];
+      run += __ldcg(&c.counts[b]);
     }
   }
   if (tid == kHistThreads - 1) c.start[nb] = run;  // total
@@ -126,26 +175,19 @@ __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const PairSou
     u32 m = 0;
     for (int w = 0; w < kHistThreads / 32; ++w) m = max(m, s_w[w]);
     c.misc[0] = m;
-    *c.gate = m > (u32)kBCap ? 1u : 0u;
+    *c.gate = m > cap ? 1u : 0u;
   }
-  // digit histograms: pass A digit = bucket & (2^TA - 1), pass B digit = bucket >> TA
-  const int TA = T - 8;
-  __shared__ u32 s_ha[256], s_hb[256];
+  // digit counts of the two passes (flushed shares and overflow moves)
   if (tid < 256) {
-    u32 hb = 0;
-    for (int b = tid << TA; b < ((tid + 1) << TA); ++b) hb += sh[b];
-    s_hb[tid] = hb;
-    u32 ha = 0;
-    if (tid < (1 << TA))
-      for (int b = tid; b < nb; b += 1 << TA) ha += sh[b];
-    s_ha[tid] = ha;
+    s_ha[tid] = __ldcg(&c.digits_a[tid]);
+    s_hb[tid] = __ldcg(&c.digits_b[tid]);
   }
   __syncthreads();
   if (tid == 0) {
     u32 ra = 0, rb = 0;
     for (int d = 0; d < 256; ++d) {
       c.bstart_a[d] = ra;
-      ra += s_ha[d];
+      ra += d < (1 << TA) ? s_ha[d] : 0u;
       c.bstart_b[d] = rb;
       rb += s_hb[d];
     }
@@ -175,22 +217,22 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) 
 // Shared-memory slot of bucket position p: one spare word per 32 keeps
 // blocked (stride-kBItems) accesses free of bank conflicts.
 __device__ __forceinline__ u32 slot(u32 p) { return p + (p >> 5); }
-constexpr int kSlots = kBCap + kBCap / 32;
 
-constexpr int kSubBits = 12;              // counting pass over the top 12 low bits
 constexpr int kSubMax = 32;               // largest sub-bucket ranked by counting
 
-struct BucketSmem {
-  static constexpr size_t bytes =
-      (size_t)kSlots * 8 * 2 + (size_t)kBWarps * kLRadix * 4 + ((size_t)1 << kSubBits) * 4 + 256;
-};
+template <class G>
+constexpr size_t bucket_smem_bytes() {
+  return (size_t)G::kSlots * 8 * 2 + (size_t)G::kBWarps * kLRadix * 4 + ((size_t)1 << G::kSubBits) * 4 + 256;
+}
 
-template <bool HW_MATCH>
-__global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
+template <class G, bool HW_MATCH>
+__global__ void __launch_bounds__(G::kBT, G::kMinBlocks) bucket_sort_collect_kernel(
     const u64* __restrict__ keys, const double* __restrict__ vals, BucketCtrl c, int T, int low_bits,
     int local_passes, int skip_zero_heads, u64* __restrict__ out_k, double* __restrict__ out_v,
     u64* __restrict__ d_nout) {
   if (gated_off(c.gate, 0)) return;  // a bucket is too large: the LSD path runs instead
+  constexpr int kBT = G::kBT, kBWarps = G::kBWarps, kBItems = G::kBItems, kIdxBits = G::kIdxBits;
+  constexpr int kSubBits = G::kSubBits, kSlots = G::kSlots;
   extern __shared__ __align__(16) unsigned char smem[];
   u64* s_x = reinterpret_cast<u64*>(smem);                       // kSlots packed words
   double* s_v = reinterpret_cast<double*>(s_x + kSlots);         // kSlots values (input order)
@@ -206,7 +248,7 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
   __syncthreads();
   const u32 b = s_misc[0];
   const u32 start = c.start[b];
-  const u32 cnt = c.start[b + 1] - start;  // <= kBCap (the gate is open)
+  const u32 cnt = c.start[b + 1] - start;  // <= G::kBCap (the gate is open)
   const u64 lowmask = (1ull << low_bits) - 1ull;
   const u32 warp_base = warp * kBItems * 32;
 
@@ -480,21 +522,29 @@ __global__ void __launch_bounds__(kBT, 2) bucket_sort_collect_kernel(
   }
 }
 
-int bucket_bits_for(u32 n) {
+// Geometry of the bucketed path: the small one when LNT_BUCKET_SMALL=1 is set
+// in the environment, else the tuned choice.
+bool small_geometry() {
+  if (const char* e = getenv("LNT_BUCKET_SMALL")) return atoi(e) != 0;
+  return kTunedBucketSmall != 0;
+}
+
+int bucket_bits_for(u32 n, bool small) {
   int lg = 0;
   while ((1u << (lg + 1)) <= n && lg < 31) ++lg;
-  return std::max(9, std::min(15, lg - 12));  // about 4096 pairs per bucket
+  return small ? std::max(9, std::min(16, lg - 11))   // about 2048 pairs per bucket
+               : std::max(9, std::min(15, lg - 12));  // about 4096 pairs per bucket
 }
 
 struct BucketLayout {
   int T;
   u32 ntiles;
-  size_t off_counts, off_start, off_ba, off_bb, off_misc, off_sa, off_sb, off_bstatus, total;
+  size_t off_counts, off_start, off_ba, off_bb, off_da, off_db, off_misc, off_sa, off_sb, off_bstatus, total;
 };
 
-BucketLayout bucket_layout(u32 n) {
+BucketLayout bucket_layout(u32 n, bool small) {
   BucketLayout L;
-  L.T = bucket_bits_for(n);
+  L.T = bucket_bits_for(n, small);
   const size_t nb = (size_t)1 << L.T;
   L.ntiles = (n + kOnesweepPassTile - 1) / kOnesweepPassTile;
   size_t off = 0;
@@ -505,6 +555,10 @@ BucketLayout bucket_layout(u32 n) {
   L.off_ba = off;
   off += 1024;
   L.off_bb = off;
+  off += 1024;
+  L.off_da = off;
+  off += 1024;
+  L.off_db = off;
   off += 1024;
   L.off_misc = off;
   off += 256;
@@ -518,13 +572,32 @@ BucketLayout bucket_layout(u32 n) {
   return L;
 }
 
+template <class G>
+int launch_bucket_sort_collect(const u64* k0, const double* v0, const BucketCtrl& c, int T, int low,
+                               int skip_zero_heads, u64* out_k, double* out_v, u64* d_nout, cudaStream_t s) {
+  constexpr size_t sh = bucket_smem_bytes<G>();
+  const int local_passes = (low + kLBits - 1) / kLBits;
+  const bool hw = getenv("LNT_BUCKET_HWMATCH") != nullptr;
+  auto kern = hw ? bucket_sort_collect_kernel<G, true> : bucket_sort_collect_kernel<G, false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
+    return LNT_DEVICE_ERROR;
+  ProfScope prof("bucket_sort_collect", s);
+  kern<<<1u << T, G::kBT, sh, s>>>(k0, v0, c, T, low, local_passes, skip_zero_heads, out_k, out_v, d_nout);
+  count_launch();
+  return launch_status();
+}
+
 }  // namespace
 
-size_t bucket_ctrl_bytes(size_t n) { return bucket_layout((u32)n).total; }
+// Scratch for either geometry (the choice can change between the workspace
+// query and the call through the environment).
+size_t bucket_ctrl_bytes(size_t n) {
+  return std::max(bucket_layout((u32)n, false).total, bucket_layout((u32)n, true).total);
+}
 
 bool bucket_path_applies(size_t n, int key_bits) {
   if (n < (1u << 20) || n >= (1u << 30)) return false;
-  const int T = bucket_bits_for((u32)n);
+  const int T = bucket_bits_for((u32)n, small_geometry());
   const int low = key_bits - T;
   return low >= 0 && low <= 4 * kLBits && key_bits > T;  // at most four local passes (41-bit packed words)
 }
@@ -535,14 +608,18 @@ bool bucket_path_applies(size_t n, int key_bits) {
 int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int skip_zero_heads, u64* k0, double* v0,
                              u64* k1, double* v1, void* ctrl, u64* out_k, double* out_v, u64* d_nout, u32* gate,
                              cudaStream_t s) {
-  const BucketLayout L = bucket_layout(n);
+  const bool small = small_geometry();
+  const BucketLayout L = bucket_layout(n, small);
   const int T = L.T, TA = T - 8, low = key_bits - T;
+  const u32 cap = small ? (u32)GeomSmall::kBCap : (u32)GeomLarge::kBCap;
   unsigned char* w = static_cast<unsigned char*>(ctrl);
   BucketCtrl c;
   c.counts = reinterpret_cast<u32*>(w + L.off_counts);
   c.start = reinterpret_cast<u32*>(w + L.off_start);
   c.bstart_a = reinterpret_cast<u32*>(w + L.off_ba);
   c.bstart_b = reinterpret_cast<u32*>(w + L.off_bb);
+  c.digits_a = reinterpret_cast<u32*>(w + L.off_da);
+  c.digits_b = reinterpret_cast<u32*>(w + L.off_db);
   c.misc = reinterpret_cast<u32*>(w + L.off_misc);
   c.status_a = reinterpret_cast<u32*>(w + L.off_sa);
   c.status_b = reinterpret_cast<u32*>(w + L.off_sb);
@@ -550,31 +627,26 @@ int run_bucketed_sort_reduce(const PairSource& src, u32 n, int key_bits, int ski
   c.gate = gate;
   if (cudaMemsetAsync(ctrl, 0, L.total, s) != cudaSuccess) return LNT_DEVICE_ERROR;
   {
-    const size_t sh = ((size_t)1 << T) * 4;
-    cudaFuncSetAttribute(bucket_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    const size_t sh = ((size_t)1 << T) * 2;  // 16-bit fields
+    if (cudaFuncSetAttribute(bucket_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
+      return LNT_DEVICE_ERROR;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bucket_hist_kernel, kHistThreads, sh) != cudaSuccess)
+      return LNT_DEVICE_ERROR;
     ProfScope prof("sort_hist", s);
-    bucket_hist_kernel<<<sm_count(), kHistThreads, sh, s>>>(src, n, T, low, c);
+    bucket_hist_kernel<<<std::max(per_sm, 1) * sm_count(), kHistThreads, sh, s>>>(src, n, T, low, cap, c);
     count_launch();
   }
   // the bucket-size decision stays on the device: the passes below return at
-  // once when the histogram found a bucket above kBCap (skewed keys)
+  // once when the histogram found a bucket above the CTA capacity (skewed keys)
   int st = run_onesweep_pass8(gated_source(src, gate, 0), true, k1, v1, n, (u32)low, (1u << TA) - 1u, c.bstart_a,
                               c.status_a, c.misc + 2, s);
   if (st != LNT_OK) return st;
   st = run_onesweep_pass8(gated_source(plain_source(k1, v1, n), gate, 0), false, k0, v0, n, (u32)(low + TA), 0xFFu,
                           c.bstart_b, c.status_b, c.misc + 3, s);
   if (st != LNT_OK) return st;
-  {
-    const size_t sh = BucketSmem::bytes;
-    const int local_passes = (low + kLBits - 1) / kLBits;
-    const bool hw = getenv("LNT_BUCKET_HWMATCH") != nullptr;
-    auto kern = hw ? bucket_sort_collect_kernel<true> : bucket_sort_collect_kernel<false>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-    ProfScope prof("bucket_sort_collect", s);
-    kern<<<1u << T, kBT, sh, s>>>(k0, v0, c, T, low, local_passes, skip_zero_heads, out_k, out_v, d_nout);
-    count_launch();
-  }
-  return launch_status();
+  return small ? launch_bucket_sort_collect<GeomSmall>(k0, v0, c, T, low, skip_zero_heads, out_k, out_v, d_nout, s)
+               : launch_bucket_sort_collect<GeomLarge>(k0, v0, c, T, low, skip_zero_heads, out_k, out_v, d_nout, s);
 }
 
 }  // namespace lnt

@@ -59,6 +59,8 @@ static const TunedSortEntry kTunedSort[] = {
 
 // digit-pass shape of the bucketed sort + collect (see run_onesweep_pass8)
 constexpr int kTunedPass8Variant = 0;
+// bucket geometry of the sort merge (0: 2^(lg n - 12) buckets, 1: 2^(lg n - 11))
+constexpr int kTunedBucketSmall = 0;
 // work-queue chunk of the batched contraction engine (units per grab)
 constexpr unsigned kTunedBatchChunk = 1;
 // dense-row threshold divisor of the tile engine

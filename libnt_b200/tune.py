@@ -102,6 +102,8 @@ def render_header(tuned: dict) -> str:
         "",
         "// digit-pass shape of the bucketed sort + collect (see run_onesweep_pass8)",
         f"constexpr int kTunedPass8Variant = {int(tuned['pass8_variant'])};",
+        "// bucket geometry of the sort merge (0: 2^(lg n - 12) buckets, 1: 2^(lg n - 11))",
+        f"constexpr int kTunedBucketSmall = {int(tuned.get('bucket_small', 0))};",
         "// work-queue chunk of the batched contraction engine (units per grab)",
         f"constexpr unsigned kTunedBatchChunk = {int(tuned['batch_chunk'])};",
         "// dense-row threshold divisor of the tile engine",
@@ -157,6 +159,32 @@ def tune_pass8(L, torch, quick=False):
                                                           out_vals=ov, count=cnt, ws=ws, sync=False))
         print(f"pass8 variant {v}: {res[v]:.3f} ms", flush=True)
     os.environ.pop("LNT_PASS8_VARIANT", None)
+    return min(res, key=res.get), res
+
+
+def tune_bucket(L, torch, quick=False):
+    """The merge of tune_pass8 at 2 x 2^26 pairs (2^25 with --quick) with the
+    large and the small bucket geometry (LNT_BUCKET_SMALL)."""
+    n = 1 << (25 if quick else 26)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    mk = 512 ** 4
+    ak = torch.randint(0, mk, (n,), generator=g, device="cuda")
+    bk = torch.randint(0, mk, (n,), generator=g, device="cuda")
+    av = torch.rand(n, generator=g, device="cuda", dtype=torch.float64)
+    bv = torch.rand(n, generator=g, device="cuda", dtype=torch.float64)
+    spec = L.RekeySpec.make([512] * 4, [0, 1, 2, 3], [3, 2, 1, 0])
+    ok = torch.empty(2 * n, dtype=torch.int64, device="cuda")
+    ov = torch.empty(2 * n, dtype=torch.float64, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ws = L.workspace(L.sort_reduce_workspace(n, n, mk))
+    res = {}
+    for small in (0, 1):
+        os.environ["LNT_BUCKET_SMALL"] = str(small)
+        res[small] = _median_ms(torch, lambda: L.sort_reduce(ak, av, bk, bv, max_key=mk, a_rekey=spec, out_keys=ok,
+                                                              out_vals=ov, count=cnt, ws=ws, sync=False))
+        print(f"bucket geometry small={small}: {res[small]:.3f} ms", flush=True)
+    os.environ.pop("LNT_BUCKET_SMALL", None)
     return min(res, key=res.get), res
 
 
@@ -234,13 +262,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--sort", action="store_true", help="onesweep variant table")
     ap.add_argument("--pass8", action="store_true", help="digit-pass shape of the bucketed sort + collect")
+    ap.add_argument("--bucket", action="store_true", help="bucket geometry of the sort merge")
     ap.add_argument("--batched", action="store_true", help="work-queue chunk of the batched engine")
     ap.add_argument("--tile", action="store_true", help="dense-row divisor of the tile engine")
     ap.add_argument("--write", action="store_true", help="merge into csrc/lnt_tuned.json and rewrite csrc/lnt_tuned.h")
     ap.add_argument("--quick", action="store_true", help="fewer and smaller cases")
     ap.add_argument("--json", default=None, help="also dump the raw timings here")
     args = ap.parse_args()
-    if not (args.sort or args.pass8 or args.batched or args.tile):
+    if not (args.sort or args.pass8 or args.bucket or args.batched or args.tile):
         args.sort = True
     sys.path.insert(0, str(PKG.parent))
     import torch
@@ -272,6 +301,8 @@ def main():
         raw["sort"] = {"variants": vs, "results": results}
     if args.pass8:
         tuned["pass8_variant"], raw["pass8"] = tune_pass8(L, torch, args.quick)
+    if args.bucket:
+        tuned["bucket_small"], raw["bucket"] = tune_bucket(L, torch, args.quick)
     if args.batched:
         tuned["batch_chunk"], raw["batched"] = tune_batched(L, torch, args.quick)
     if args.tile:

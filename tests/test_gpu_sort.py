@@ -177,7 +177,7 @@ def test_sort_merge_matches_oracle(cuda, torch, rng, dims, na, nb, op):
     assert cuda.device_status() == 0
 
 
-@pytest.mark.parametrize("path", ["bucketed", "lsd"])
+@pytest.mark.parametrize("path", ["bucketed", "bucketed_small", "lsd"])
 @pytest.mark.parametrize("dims,n_each,dup_frac", [([512] * 4, 1 << 20, 0.0), ([64] * 4, 1 << 20, 0.0),
                                                    ([512] * 4, 3 << 19, 0.0), ([512] * 4, 1 << 20, 0.5)])
 def test_sort_merge_both_paths(cuda, torch, rng, monkeypatch, path, dims, n_each, dup_frac):
@@ -187,6 +187,7 @@ def test_sort_merge_both_paths(cuda, torch, rng, monkeypatch, path, dims, n_each
     import libnt_b200 as L
     if path == "lsd":
         monkeypatch.setenv("LNT_NO_BUCKETS", "1")
+    monkeypatch.setenv("LNT_BUCKET_SMALL", "1" if path == "bucketed_small" else "0")
     ak, av, bk, bv = _merge_case(rng, dims, n_each, n_each, zero_frac=0.1)
     if dup_frac:
         ak[: int(n_each * dup_frac)] = ak[0]
