@@ -57,10 +57,12 @@ LNT_API int lnt_mex_sparse_merge(const double* a_vals, const int64_t* a_keys, si
 /* SparseLatticeMultMex(a_vals, a_keys, a_dims, b_vals, b_keys, b_dims, alg)
  * (MATLAB/mex/sparselattice_mul.cpp:14-137): A (a_dims = [h w d]) and B
  * ([w wB d]) key-sorted column-major; C = A * B per tab (csc_no_accum: keys
- * ascending, exact zero sums kept).  alg 0 (operator*) and 3 (CSCNA) are this
- * product; the other algorithms (csc_times, DCSC, outer and mtt products)
- * return LNT_UNSUPPORTED.  LNT_BAD_DIMS when a_dims[1] != b_dims[0] or the
- * depths differ. */
+ * ascending, exact zero sums kept).  alg 0 (operator*), 1 (CSC: csc_times),
+ * 2 (DCSC) and 3 (CSCNA) all compute this product with this pattern; alg 4
+ * and 5 return LNT_UNSUPPORTED: in the reference both reach mtt_times (alg 4
+ * falls through into 5), whose body computes and returns nothing
+ * (SparseLatticeBase.h:1582-1640).  LNT_BAD_DIMS when a_dims[1] != b_dims[0]
+ * or the depths differ. */
 LNT_API int lnt_mex_sparselattice_mult(const double* a_vals, const int64_t* a_keys, size_t na,
                                        const int64_t* a_dims, const double* b_vals, const int64_t* b_keys,
                                        size_t nb, const int64_t* b_dims, int alg, lnt_host_alloc alloc,

@@ -188,7 +188,12 @@ int lnt_mex_sparselattice_mult(const double* a_vals, const int64_t* a_keys, size
                                const double* b_vals, const int64_t* b_keys, size_t nb, const int64_t* b_dims,
                                int alg, lnt_host_alloc alloc, double** c_vals, int64_t** c_keys, size_t* nc) {
   if (!nc || !a_dims || !b_dims || (na && !a_vals) || (nb && !b_vals)) return LNT_BAD_ARG;
-  if (alg != 0 && alg != 3) return LNT_UNSUPPORTED;
+  // 0 operator*, 1 csc_times<false>, 2 csc_times<true> (DCSC), 3 csc_no_accum: the
+  // same product with the same pattern (zero sums kept) in column-major order.
+  // 4 and 5 reach mtt_times (4 falls through into 5, sparselattice_mul.cpp:52-62),
+  // whose body ends after its declarations without computing or returning a
+  // result (SparseLatticeBase.h:1582-1640): nothing to reproduce.
+  if (alg < 0 || alg > 3) return LNT_UNSUPPORTED;
   if (a_dims[1] != b_dims[0] || a_dims[2] != b_dims[2]) return LNT_BAD_DIMS;
   int st = check_keys(a_keys, na, nullptr);
   if (st != LNT_OK || (st = check_keys(b_keys, nb, nullptr)) != LNT_OK) return st;

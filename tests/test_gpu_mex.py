@@ -89,8 +89,11 @@ def test_mex_merge(lib, rng, op, use_malloc):
     np.testing.assert_array_equal(v, ev)
 
 
-@pytest.mark.parametrize("alg", [0, 3])
+@pytest.mark.parametrize("alg", [0, 1, 2, 3])
 def test_mex_sparselattice_mult(lib, rng, alg):
+    """Algorithms 0 (operator*), 1 (csc_times), 2 (DCSC) and 3 (csc_no_accum)
+    give the same product and pattern; 1 and 2 are also checked against the
+    csc_times restatement."""
     h, w, wB, d = 60, 50, 40, 3
     ak = np.unique(rng.integers(0, h * w * d, 3000)).astype(np.int64)
     bk = np.unique(rng.integers(0, w * wB * d, 2000)).astype(np.int64)
@@ -101,6 +104,25 @@ def test_mex_sparselattice_mult(lib, rng, alg):
     ek, ev, ea = oracle.lattice_mult(ak.astype(np.uint64), av, h, w, d, bk.astype(np.uint64), bv, wB, with_abs=True)
     np.testing.assert_array_equal(k, ek)
     assert np.all(np.abs(v - ev) <= 1e-12 * ea)
+    if alg in (1, 2):
+        ck, cv = oracle.csc_times(ak.astype(np.uint64), av, h, w, d, bk.astype(np.uint64), bv, wB)
+        np.testing.assert_array_equal(k, ck)
+        assert np.all(np.abs(v - cv) <= 1e-12 * ea)
+
+
+@pytest.mark.parametrize("alg", [4, 5, -1, 6])
+def test_mex_sparselattice_mult_unavailable_algorithms(lib, alg):
+    """4 and 5 reach the reference's unfinished mtt_times; out-of-range values
+    are rejected too: LNT_UNSUPPORTED, nothing allocated or returned."""
+    import ctypes as C
+    ak = np.array([0, 5], np.int64)
+    av = np.array([1.0, 2.0])
+    ad = np.array([3, 4, 1], np.int64)
+    bd = np.array([4, 2, 1], np.int64)
+    cv, ck, nc = C.c_void_p(), C.c_void_p(), C.c_size_t(7)
+    st = lib.lnt_mex_sparselattice_mult(ptr(av), ptr(ak), 2, ptr(ad), ptr(av), ptr(ak), 2, ptr(bd), alg, None,
+                                        C.byref(cv), C.byref(ck), C.byref(nc))
+    assert st == 8
 
 
 @pytest.mark.parametrize("dense_first", [True, False])
