@@ -92,8 +92,8 @@ def test_mex_gateways_reject_bad_arguments_without_gpu():
     d3 = np.array([4, 5, 1], np.int64)
     e3 = np.array([6, 2, 1], np.int64)   # rows(B) != cols(A)
     args = (vals.ctypes.data, keys.ctypes.data, 3, d3.ctypes.data, vals.ctypes.data, keys.ctypes.data, 3)
-    assert lib.lnt_mex_sparselattice_mult(*args, d3.ctypes.data, 1, L.HostAlloc(), C.byref(cv), C.byref(ck),
-                                          C.byref(nc)) == 8   # csc_times: not this product
+    assert lib.lnt_mex_sparselattice_mult(*args, d3.ctypes.data, 5, L.HostAlloc(), C.byref(cv), C.byref(ck),
+                                          C.byref(nc)) == 8   # mtt_times: the reference computes nothing
     assert lib.lnt_mex_sparselattice_mult(*args, e3.ctypes.data, 0, L.HostAlloc(), C.byref(cv), C.byref(ck),
                                           C.byref(nc)) == 2
     B = np.ones(12)
