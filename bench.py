@@ -801,12 +801,13 @@ def run_batched(args):
         kernels[name] = {"ms_total": t, "launches": c}
     L.profile_reset()
     g = torch.cuda.CUDAGraph()
+    c0 = L.launch_count()
     with torch.cuda.graph(g):
         batch.run()
+    per_replay = L.launch_count() - c0  # kernels recorded into the graph (a replay does not pass the host counter)
     for _ in range(args.warmup):
         g.replay()
     torch.cuda.synchronize()
-    launches0 = L.launch_count()
     e0, e1 = _events()
     sampler = ClockSampler(torch.cuda.current_device())
     with sampler:
@@ -816,7 +817,7 @@ def run_batched(args):
         e1.record()
         torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
-    launches = L.launch_count() - launches0
+    launches = per_replay * args.steps
     assert L.device_status() == 0, "device-side wait expired"
     out_total = int(batch.c_off[-1].item())
     # products per problem: over B entries, the size of the A column they meet
