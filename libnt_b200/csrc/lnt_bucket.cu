@@ -243,8 +243,12 @@ __global__ void __launch_bounds__(G::kBT, G::kMinBlocks) bucket_sort_collect_ker
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const u32 nb = 1u << T;
+  const int sb_bits = min(low_bits, kSubBits);
+  const int nsb = 1 << sb_bits;
+  const int sb_shift = kIdxBits + low_bits - sb_bits;
   if (tid == 0) s_misc[0] = atomicAdd(&c.misc[4], 1u);
   for (int x = tid; x < kBWarps * kLRadix; x += kBT) s_whist[x] = 0;
+  for (int x = tid; x < nsb; x += kBT) s_sub[x] = 0;  // counting pass below
   __syncthreads();
   const u32 b = s_misc[0];
   const u32 start = c.start[b];
@@ -272,11 +276,6 @@ __global__ void __launch_bounds__(G::kBT, G::kMinBlocks) bucket_sort_collect_ker
   // sub-bucket counts places every word; each word then finds its rank among
   // the (few) words of its sub-bucket by the whole packed word, i.e. by key
   // and then by input index, so the result is the stable order.
-  const int sb_bits = min(low_bits, kSubBits);
-  const int nsb = 1 << sb_bits;
-  const int sb_shift = kIdxBits + low_bits - sb_bits;
-  for (int x = tid; x < nsb; x += kBT) s_sub[x] = 0;
-  __syncthreads();
   u32 rnk[kBItems];
 #pragma unroll
   for (int i = 0; i < kBItems; ++i) {
@@ -352,7 +351,8 @@ __global__ void __launch_bounds__(G::kBT, G::kMinBlocks) bucket_sort_collect_ker
 #pragma unroll
     for (int i = 0; i < kBItems; ++i)
       if (rnk[i] != ~0u) s_x[slot(rnk[i])] = w[i];
-    __syncthreads();
+    asm volatile("cp.async.wait_all;\n" ::: "memory");  // this thread's value copies have landed
+    __syncthreads();                                    // ... and everyone's, for the fold
   } else {
   // ---- clustered keys: local LSD passes over the low bits -----------------------
   const u32 lt_mask = (1u << lane) - 1u;
@@ -409,6 +409,7 @@ __global__ void __launch_bounds__(G::kBT, G::kMinBlocks) bucket_sort_collect_ker
       const u32 p = warp_base + i * 32 + lane;
       if (p < cnt) s_x[slot(pos[i])] = w[i];
     }
+    if (q + 1 == local_passes) asm volatile("cp.async.wait_all;\n" ::: "memory");  // values, for the fold
     __syncthreads();
     if (q + 1 < local_passes) {
 #pragma unroll
@@ -421,8 +422,6 @@ __global__ void __launch_bounds__(G::kBT, G::kMinBlocks) bucket_sort_collect_ker
     }
   }
   }  // clustered keys
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();  // every thread's value copies have landed
 
   // ---- fold runs of equal keys (they all lie in this bucket) ------------------
   const u64 prefix = (u64)b << low_bits;

@@ -114,7 +114,7 @@ int make_rekey_params(int order, const int64_t* dims, const int32_t* cur_seq,
                       const int32_t* new_seq, RekeyParams* out) {
   if (!out) return LNT_BAD_ARG;
   out->order = 0;
-  out->pad = 0;
+  out->pow2 = 0;
   if (order <= 1) return order < 0 ? LNT_BAD_ARG : LNT_OK;
   if (order > LNT_MAX_ORDER || !dims || !cur_seq || !new_seq) return LNT_BAD_ARG;
   if (!is_permutation(order, cur_seq) || !is_permutation(order, new_seq)) return LNT_BAD_SEQ;
@@ -142,6 +142,18 @@ int make_rekey_params(int order, const int64_t* dims, const int32_t* cur_seq,
   }
   for (int i = 0; i < order; ++i) out->mult[i] = stride_of_mode[cur_seq[i]];
   out->order = order;
+  bool pow2 = true;
+  for (int i = 0; i < order; ++i) pow2 = pow2 && ((u64)dims[i] & ((u64)dims[i] - 1)) == 0;
+  out->pow2 = pow2 ? 1 : 0;
+  for (int i = 0; i < LNT_MAX_ORDER; ++i) out->field[i] = 0;
+  if (pow2) {
+    for (int i = 0; i < order; ++i) {
+      const u32 src = (u32)__builtin_ctzll(out->acc[i].d);
+      const u32 bits = (u32)__builtin_ctzll((u64)dims[cur_seq[i]]);
+      const u32 dst = (u32)__builtin_ctzll(out->mult[i]);
+      out->field[i] = src | (bits << 8) | (dst << 16);
+    }
+  }
   return LNT_OK;
 }
 

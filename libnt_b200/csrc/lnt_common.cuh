@@ -157,13 +157,38 @@ __host__ __device__ __forceinline__ u64 divide(u64 n, const Divider& dv) {
 // ---------------------------------------------------------------------------
 struct RekeyParams {
   int order;        // 0 or 1 => identity
-  int pad;
+  int pow2;         // every extent a power of two: `field` holds the bit-field moves
   Divider acc[LNT_MAX_ORDER];  // cumulative extents, current order
   u64 mult[LNT_MAX_ORDER];     // new stride of the mode at current position i
+  u32 field[LNT_MAX_ORDER];    // pow2: source shift | bits << 8 | destination shift << 16
 };
+
+// With power-of-two extents the re-key is a permutation of bit fields: the
+// mode at current position i occupies `bits` bits at its cumulative-extent
+// shift and moves to its new stride's shift.
+template <int N>
+__host__ __device__ __forceinline__ u64 rekey_fields(u64 k, const RekeyParams& p) {
+  u64 out = 0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const u32 f = p.field[i];
+    out |= ((k >> (f & 63u)) & ((1ull << ((f >> 8) & 63u)) - 1ull)) << ((f >> 16) & 63u);
+  }
+  return out;
+}
 
 __host__ __device__ __forceinline__ u64 rekey(u64 k, const RekeyParams& p) {
   if (p.order <= 1) return k;
+  if (p.pow2) {
+    switch (p.order) {
+      case 2: return rekey_fields<2>(k, p);
+      case 3: return rekey_fields<3>(k, p);
+      case 4: return rekey_fields<4>(k, p);
+      case 5: return rekey_fields<5>(k, p);
+      case 6: return rekey_fields<6>(k, p);
+      default: break;
+    }
+  }
   u64 out = 0;
 #pragma unroll 1
   for (int i = p.order - 1; i >= 1; --i) {
