@@ -120,8 +120,9 @@ def test_mex_sparselattice_mult_unavailable_algorithms(lib, alg):
     ad = np.array([3, 4, 1], np.int64)
     bd = np.array([4, 2, 1], np.int64)
     cv, ck, nc = C.c_void_p(), C.c_void_p(), C.c_size_t(7)
-    st = lib.lnt_mex_sparselattice_mult(ptr(av), ptr(ak), 2, ptr(ad), ptr(av), ptr(ak), 2, ptr(bd), alg, None,
-                                        C.byref(cv), C.byref(ck), C.byref(nc))
+    import libnt_b200 as L
+    st = lib.lnt_mex_sparselattice_mult(ptr(av), ptr(ak), 2, ptr(ad), ptr(av), ptr(ak), 2, ptr(bd), alg,
+                                        L.HostAlloc(), C.byref(cv), C.byref(ck), C.byref(nc))
     assert st == 8
 
 
