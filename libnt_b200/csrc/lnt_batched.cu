@@ -76,31 +76,44 @@ __device__ __forceinline__ int find_problem_by_unit(const ProbDesc* prob, int co
 }
 
 // Column pointers of every problem's A (which == 0) or B (which == 1).
-// Position q enumerates, problem by problem, the n_p + 1 boundaries; each
-// thread takes 8 consecutive positions (one binary search for the problem).
+// Position q enumerates, problem by problem, the n_p + 1 boundaries; position
+// i of problem p fills the pointer entries of the (possibly many empty)
+// columns between entry i-1's column and entry i's.  A warp takes 32
+// consecutive positions and fills their ranges together, lane by lane over
+// the columns, so a long run of empty columns is written by the whole warp in
+// coalesced stores instead of by one thread.
 __global__ void batch_colptr_kernel(BatchArgs args, int which, const u64* __restrict__ pos_off, u64 total_pos) {
-  constexpr u64 kPer = 8;
-  const u64 stride = (u64)gridDim.x * blockDim.x * kPer;
-  for (u64 q0 = ((u64)blockIdx.x * blockDim.x + threadIdx.x) * kPer; q0 < total_pos; q0 += stride) {
-    int lo = 0, hi = args.count - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (pos_off[mid] <= q0) lo = mid; else hi = mid - 1;
-    }
-    int p = lo;
-    const u64 q1 = min(q0 + kPer, total_pos);
-    for (u64 q = q0; q < q1; ++q) {
-      while (p + 1 < args.count && pos_off[p + 1] <= q) ++p;
-      const ProbDesc& P = args.prob[p];
-      const u64 i = q - pos_off[p];
+  const int lane = threadIdx.x & 31;
+  const u64 warps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 q0 = (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; q0 < total_pos; q0 += warps * 32) {
+    const u64 q = q0 + lane;
+    const bool valid = q < total_pos;
+    long long prev = 0, cur = -1;
+    u32 idx = 0;
+    unsigned long long base = 0;
+    if (valid) {
+      int lo = 0, hi = args.count - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pos_off[mid] <= q) lo = mid; else hi = mid - 1;
+      }
+      const ProbDesc& P = args.prob[lo];
+      const u64 i = q - pos_off[lo];
       const u64 n = which == 0 ? P.a_n : P.b_n;
       const u64* keys = which == 0 ? args.ak + P.a_off : args.bk + P.b_off;
       const Divider& dv = which == 0 ? P.div_h : P.div_w;
       const u64 ncol = which == 0 ? P.w * P.d : P.units;
-      u32* ptr = (which == 0 ? args.aptr + P.aptr_off : args.bptr + P.bptr_off);
-      const long long prev = i == 0 ? -1ll : (long long)min(divide(keys[i - 1] & args.kmask, dv), ncol);
-      const u64 cur = i == n ? ncol : min(divide(keys[i] & args.kmask, dv), ncol);
-      for (long long c = prev + 1; c <= (long long)cur; ++c) ptr[c] = (u32)i;
+      prev = i == 0 ? -1ll : (long long)min(divide(keys[i - 1] & args.kmask, dv), ncol);
+      cur = i == n ? (long long)ncol : (long long)min(divide(keys[i] & args.kmask, dv), ncol);
+      idx = (u32)i;
+      base = (unsigned long long)(which == 0 ? args.aptr + P.aptr_off : args.bptr + P.bptr_off);
+    }
+    for (int j = 0; j < 32; ++j) {
+      const long long pj = __shfl_sync(0xffffffffu, prev, j);
+      const long long cj = __shfl_sync(0xffffffffu, cur, j);
+      const u32 ij = __shfl_sync(0xffffffffu, idx, j);
+      u32* ptr = reinterpret_cast<u32*>(__shfl_sync(0xffffffffu, base, j));
+      for (long long c = pj + 1 + lane; c <= cj; c += 32) ptr[c] = ij;
     }
   }
 }
@@ -380,9 +393,9 @@ int run_batch_product(const BatchArgs& args, const BatchLayout& L, unsigned char
   if (cudaMemsetAsync(queue, 0, 256, s) != cudaSuccess) return LNT_DEVICE_ERROR;
   {
     ProfScope prof("batch_colptr", s);
-    const int ga = (int)std::max<u64>(1, std::min<u64>((L.a_pos / 8 + 255) / 256, (u64)sms * 16));
+    const int ga = (int)std::max<u64>(1, std::min<u64>((L.a_pos + 255) / 256, (u64)sms * 16));
     batch_colptr_kernel<<<ga, 256, 0, s>>>(args, 0, reinterpret_cast<const u64*>(w + L.off_apos), L.a_pos);
-    const int gb = (int)std::max<u64>(1, std::min<u64>((L.b_pos / 8 + 255) / 256, (u64)sms * 16));
+    const int gb = (int)std::max<u64>(1, std::min<u64>((L.b_pos + 255) / 256, (u64)sms * 16));
     batch_colptr_kernel<<<gb, 256, 0, s>>>(args, 1, reinterpret_cast<const u64*>(w + L.off_bpos), L.b_pos);
     count_launch(2);
   }
