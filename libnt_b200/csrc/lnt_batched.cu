@@ -78,42 +78,59 @@ __device__ __forceinline__ int find_problem_by_unit(const ProbDesc* prob, int co
 // Column pointers of every problem's A (which == 0) or B (which == 1).
 // Position q enumerates, problem by problem, the n_p + 1 boundaries; position
 // i of problem p fills the pointer entries of the (possibly many empty)
-// columns between entry i-1's column and entry i's.  A warp takes 32
-// consecutive positions and fills their ranges together, lane by lane over
-// the columns, so a long run of empty columns is written by the whole warp in
-// coalesced stores instead of by one thread.
+// columns between entry i-1's column and entry i's.  Each thread takes 8
+// consecutive positions (one binary search for the problem) and fills short
+// ranges itself; a range longer than kLongRun columns (a run of empty columns,
+// common in problems with far more columns than entries) is filled by the
+// whole warp together in coalesced stores, so no thread writes a long run
+// alone.
 __global__ void batch_colptr_kernel(BatchArgs args, int which, const u64* __restrict__ pos_off, u64 total_pos) {
+  constexpr u64 kPer = 8;
+  constexpr long long kLongRun = 32;
   const int lane = threadIdx.x & 31;
   const u64 warps = ((u64)gridDim.x * blockDim.x) >> 5;
-  for (u64 q0 = (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; q0 < total_pos; q0 += warps * 32) {
-    const u64 q = q0 + lane;
-    const bool valid = q < total_pos;
-    long long prev = 0, cur = -1;
-    u32 idx = 0;
-    unsigned long long base = 0;
-    if (valid) {
+  const u64 warp_id = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (u64 w0 = warp_id * 32 * kPer; w0 < total_pos; w0 += warps * 32 * kPer) {
+    const u64 q0 = w0 + (u64)lane * kPer;
+    int p = 0;
+    if (q0 < total_pos) {
       int lo = 0, hi = args.count - 1;
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (pos_off[mid] <= q) lo = mid; else hi = mid - 1;
+        if (pos_off[mid] <= q0) lo = mid; else hi = mid - 1;
       }
-      const ProbDesc& P = args.prob[lo];
-      const u64 i = q - pos_off[lo];
-      const u64 n = which == 0 ? P.a_n : P.b_n;
-      const u64* keys = which == 0 ? args.ak + P.a_off : args.bk + P.b_off;
-      const Divider& dv = which == 0 ? P.div_h : P.div_w;
-      const u64 ncol = which == 0 ? P.w * P.d : P.units;
-      prev = i == 0 ? -1ll : (long long)min(divide(keys[i - 1] & args.kmask, dv), ncol);
-      cur = i == n ? (long long)ncol : (long long)min(divide(keys[i] & args.kmask, dv), ncol);
-      idx = (u32)i;
-      base = (unsigned long long)(which == 0 ? args.aptr + P.aptr_off : args.bptr + P.bptr_off);
+      p = lo;
     }
-    for (int j = 0; j < 32; ++j) {
-      const long long pj = __shfl_sync(0xffffffffu, prev, j);
-      const long long cj = __shfl_sync(0xffffffffu, cur, j);
-      const u32 ij = __shfl_sync(0xffffffffu, idx, j);
-      u32* ptr = reinterpret_cast<u32*>(__shfl_sync(0xffffffffu, base, j));
-      for (long long c = pj + 1 + lane; c <= cj; c += 32) ptr[c] = ij;
+    for (u64 k = 0; k < kPer; ++k) {
+      const u64 q = q0 + k;
+      long long prev = 0, cur = -1;
+      u32 idx = 0;
+      u32* ptr = nullptr;
+      if (q < total_pos) {
+        while (p + 1 < args.count && pos_off[p + 1] <= q) ++p;
+        const ProbDesc& P = args.prob[p];
+        const u64 i = q - pos_off[p];
+        const u64 n = which == 0 ? P.a_n : P.b_n;
+        const u64* keys = which == 0 ? args.ak + P.a_off : args.bk + P.b_off;
+        const Divider& dv = which == 0 ? P.div_h : P.div_w;
+        const u64 ncol = which == 0 ? P.w * P.d : P.units;
+        ptr = which == 0 ? args.aptr + P.aptr_off : args.bptr + P.bptr_off;
+        prev = i == 0 ? -1ll : (long long)min(divide(keys[i - 1] & args.kmask, dv), ncol);
+        cur = i == n ? (long long)ncol : (long long)min(divide(keys[i] & args.kmask, dv), ncol);
+        idx = (u32)i;
+        if (cur - prev <= kLongRun)
+          for (long long c = prev + 1; c <= cur; ++c) ptr[c] = idx;
+      }
+      u32 longm = __ballot_sync(0xffffffffu, cur - prev > kLongRun);
+      while (longm) {
+        const int j = __ffs(longm) - 1;
+        longm &= longm - 1u;
+        const long long pj = __shfl_sync(0xffffffffu, prev, j);
+        const long long cj = __shfl_sync(0xffffffffu, cur, j);
+        const u32 ij = __shfl_sync(0xffffffffu, idx, j);
+        u32* pp = reinterpret_cast<u32*>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(ptr), j));
+        for (long long c = pj + 1 + lane; c <= cj; c += 32) pp[c] = ij;
+      }
     }
   }
 }
@@ -393,9 +410,9 @@ int run_batch_product(const BatchArgs& args, const BatchLayout& L, unsigned char
   if (cudaMemsetAsync(queue, 0, 256, s) != cudaSuccess) return LNT_DEVICE_ERROR;
   {
     ProfScope prof("batch_colptr", s);
-    const int ga = (int)std::max<u64>(1, std::min<u64>((L.a_pos + 255) / 256, (u64)sms * 16));
+    const int ga = (int)std::max<u64>(1, std::min<u64>((L.a_pos / 8 + 255) / 256, (u64)sms * 16));
     batch_colptr_kernel<<<ga, 256, 0, s>>>(args, 0, reinterpret_cast<const u64*>(w + L.off_apos), L.a_pos);
-    const int gb = (int)std::max<u64>(1, std::min<u64>((L.b_pos + 255) / 256, (u64)sms * 16));
+    const int gb = (int)std::max<u64>(1, std::min<u64>((L.b_pos / 8 + 255) / 256, (u64)sms * 16));
     batch_colptr_kernel<<<gb, 256, 0, s>>>(args, 1, reinterpret_cast<const u64*>(w + L.off_bpos), L.b_pos);
     count_launch(2);
   }
