@@ -488,6 +488,33 @@ def run_ours(args):
     if m != n_out or not (np.array_equal(lanes[0].hok[:m].numpy(), out_k[:m].cpu().numpy())
                           and np.array_equal(lanes[0].hov[:m].numpy(), out_v[:m].cpu().numpy())):
         raise RuntimeError("end-to-end merge result differs from the device-resident one")
+
+    # the same copies without the merge: the PCIe floor of an e2e step
+    def copy_step(i):
+        ln = lanes[i % len(lanes)]
+        with torch.cuda.stream(ln.stream):
+            for d, h in zip(ln.din, hin):
+                d.copy_(h, non_blocking=True)
+            ln.hcnt.copy_(ln.cnt, non_blocking=True)
+            ln.hok.copy_(ln.ok, non_blocking=True)
+            ln.hov.copy_(ln.ov, non_blocking=True)
+
+    for i in range(len(lanes)):
+        copy_step(i)
+    torch.cuda.synchronize()
+    barrier(world)
+    f0.record(stream)
+    for ln in lanes:
+        ln.stream.wait_event(f0)
+    for i in range(e2e_steps):
+        copy_step(i)
+    for ln in lanes:
+        ev = torch.cuda.Event()
+        ev.record(ln.stream)
+        stream.wait_event(ev)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    copy_ms = max_over_ranks(f0.elapsed_time(f1) / e2e_steps, world)
     del lanes
     torch.cuda.empty_cache()
 
@@ -547,7 +574,9 @@ def run_ours(args):
             "oracle_check": check,
             "e2e": {"value": e2e_value, "unit": "nnz/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(16 * n + 8),
-                    "pipelining": f"{E2E_LANES} streams: the H2D of steps i+1, i+2 overlap step i's merge and D2H"},
+                    "pipelining": f"{E2E_LANES} streams: the H2D of steps i+1, i+2 overlap step i's merge and D2H",
+                    "copy_only_ms_per_step": copy_ms,
+                    "copy_only_note": "the same H2D and D2H copies per step with no merge (PCIe floor of a step)"},
             "gpu_launches": launches,
             "step_alg_bytes": step_alg, "step_hbm_frac_alg": step_alg / (ms * 1e-3) / 1e9 / peak,
             "kernels": kernels,
