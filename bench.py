@@ -1008,7 +1008,8 @@ def measure_dense(args):
             t_crt = timed(lambda: L.dense_mult_crt(A, B, n, n, n, 1, moduli, out=Cc, ws=wsc))
         L.profile_enable(False)
         kern = {k: L.profile_query(k)[0] / (reps + max(1, args.warmup // 3))
-                for k in ("dense_residues", "dense_mod_gemm", "dense_crt")}
+                for k in ("dense_residues", "dense_exp_a", "dense_exp_b", "dense_residue_a", "dense_residue_b",
+                          "dense_mod_gemm", "dense_crt")}
         L.profile_reset()
         del wsc
         torch.cuda.empty_cache()

@@ -849,18 +849,30 @@ int lnt_dense_lattice_mult_crt(const double* A, const double* B, double* C, int6
       ProfScope prof("dense_residues", s);
       const u64 kchunk = 256;
       fill_int_kernel<<<(unsigned)((uh + 255) / 256), 256, 0, s>>>(eA, uh, -4096);  // below any double exponent
-      row_exp_chunk_kernel<<<dim3((unsigned)((uh + 255) / 256), (unsigned)((uw + kchunk - 1) / kchunk)), 256, 0, s>>>(
-          At, uh, uw, kchunk, eA);
-      col_exp_kernel<<<(unsigned)((uwB * 32 + 255) / 256), 256, 0, s>>>(Bt, uw, uwB, eB);
+      {
+        ProfScope prof_a("dense_exp_a", s);
+        row_exp_chunk_kernel<<<dim3((unsigned)((uh + 255) / 256), (unsigned)((uw + kchunk - 1) / kchunk)), 256, 0,
+                               s>>>(At, uh, uw, kchunk, eA);
+      }
+      {
+        ProfScope prof_b("dense_exp_b", s);
+        col_exp_kernel<<<(unsigned)((uwB * 32 + 255) / 256), 256, 0, s>>>(Bt, uw, uwB, eB);
+      }
       if (Kp != uw || L.Mp != uh || L.Np != uwB) {  // zero every padding row and column
         if (cudaMemsetAsync(ra, 0, (u64)moduli * L.Mp * Kp, s) != cudaSuccess) return LNT_DEVICE_ERROR;
         if (cudaMemsetAsync(rb, 0, (u64)moduli * L.Np * Kp, s) != cudaSuccess) return LNT_DEVICE_ERROR;
       }
-      residue_a_kernel<<<dim3((unsigned)((uh + 31) / 32), (unsigned)((Kp + 127) / 128)), 256, 0, s>>>(
-          At, uh, uw, L.Mp, Kp, eA, P, ra);
+      {
+        ProfScope prof_ra("dense_residue_a", s);
+        residue_a_kernel<<<dim3((unsigned)((uh + 31) / 32), (unsigned)((Kp + 127) / 128)), 256, 0, s>>>(
+            At, uh, uw, L.Mp, Kp, eA, P, ra);
+      }
       const unsigned gx = (unsigned)std::min<u64>((Kp / 4 + 255) / 256, 64);
       const unsigned gyb = (unsigned)std::min<u64>(uwB, std::max<u64>(1, (u64)sms * 64 / gx));
-      residue_b_kernel<<<dim3(gx, gyb), 256, 0, s>>>(Bt, uw, uwB, L.Np, Kp, eB, P, rb);
+      {
+        ProfScope prof_rb("dense_residue_b", s);
+        residue_b_kernel<<<dim3(gx, gyb), 256, 0, s>>>(Bt, uw, uwB, L.Np, Kp, eB, P, rb);
+      }
       count_launch(5);
     }
     // all moduli's products on the tensor cores, reduced modulo m_l in the epilogue

@@ -54,7 +54,8 @@ struct ModGemmArgs {
   int nmod;
   int tiles_m, tiles_n;
   int mod[24];
-  float inv_mod[24];
+  u32 off[24];     // m ceil(2^31 / m): makes a product non-negative without changing its residue
+  u64 magic[24];   // floor(2^64 / m) + 1
   unsigned char* out;   // nmod planes of Mp x Np bytes, column-major
 };
 
@@ -174,18 +175,16 @@ __device__ __forceinline__ void tile_coords(int t, const ModGemmArgs& a, int& l,
   tn = band * kGroupN + (r - tm * width);
 }
 
-// P mod m in [0, m) for |P| < 2^31, m <= 256: the float quotient of P is off
-// by at most 3 (three roundings of relative size 2^-24), so r = P - q m lies
-// within 4m of zero; a second quotient of that small, exactly representable r
-// leaves r in [-1, m], and one correction each way finishes.
-__device__ __forceinline__ u32 mod_small(int p, int m, float inv_m) {
-  int q = __float2int_rd(__int2float_rn(p) * inv_m);
-  int r = p - q * m;
-  q = __float2int_rd(__int2float_rn(r) * inv_m);
-  r -= q * m;
-  r += r < 0 ? m : 0;
-  r -= r >= m ? m : 0;
-  return (u32)r;
+// P mod m in [0, m) for |P| < 2^31 - 2^18 (so Kp < 2^17): u = P + off with
+// off = m ceil(2^31 / m) is congruent to P and lies in [0, 2^32); then
+// q = floor(u M / 2^64) with M = floor(2^64 / m) + 1 is floor(u / m) exactly,
+// since u M / 2^64 exceeds u / m by less than u / 2^64 < 2^-32 < 1/m and the
+// fraction of u / m is at most 1 - 1/m (division by an invariant integer,
+// Granlund & Montgomery 1994); r = u - q m.
+__device__ __forceinline__ u32 mod_small(int p, u32 m, u32 off, u64 magic) {
+  const u32 u = (u32)p + off;
+  const u32 q = (u32)__umul64hi((u64)u, magic);
+  return u - q * m;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) mod_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
@@ -314,8 +313,8 @@ __global__ void __launch_bounds__(kThreads, 1) mod_gemm_kernel(const __grid_cons
       const int got = lane == 0 ? (int)mbar_wait(tfull, (u32)(it & 1), abort_flag) : 0;
       if (!__shfl_sync(0xffffffffu, got, 0)) break;
       tc_fence_after();
-      const int m = args.mod[l];
-      const float inv_m = args.inv_mod[l];
+      const u32 m = (u32)args.mod[l], off = args.off[l];
+      const u64 magic = args.magic[l];
       unsigned char* plane = args.out + (size_t)l * args.Mp * args.Np;
 #pragma unroll 1
       for (int mb = 0; mb < 2; ++mb) {
@@ -329,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1) mod_gemm_kernel(const __grid_cons
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const u64 col = col0 + j;
-            if (row < args.Mp && col < args.Np) plane[row + args.Mp * col] = (unsigned char)mod_small((int)v[j], m, inv_m);
+            if (row < args.Mp && col < args.Np) plane[row + args.Mp * col] = (unsigned char)mod_small((int)v[j], m, off, magic);
           }
         }
       }
@@ -396,7 +395,9 @@ int run_mod_gemm(const signed char* ra, const signed char* rb, int nmod, const i
   a.tiles_n = (int)((Np + kBN - 1) / kBN);
   for (int l = 0; l < 24; ++l) {
     a.mod[l] = l < nmod ? moduli[l] : 1;
-    a.inv_mod[l] = 1.0f / (float)a.mod[l];
+    const u64 m = (u64)a.mod[l];
+    a.off[l] = (u32)(m * (((1ull << 31) + m - 1) / m));
+    a.magic[l] = (u64)(~0ull / m) + (m == 1 ? 0ull : 1ull);  // floor(2^64 / m) + 1 (m = 1: any q works)
   }
   a.out = out;
   CUtensorMap ma, mb;
