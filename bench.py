@@ -531,6 +531,15 @@ def run_ours(args):
         "bucket_sort_collect": ("per-bucket shared-memory sort + duplicate fold of the 2^27 pairs",
                                 16.0 * n + 16.0 * n_out, "bucket_traffic_bytes_per_pair"),
     }
+    # every timed merge kernel's algorithmic bytes and fraction of the HBM peak
+    per_launch_bytes = {"sort_hist": 8.0 * n, "sort_onesweep": 32.0 * n,
+                        "bucket_sort_collect": 16.0 * n + 16.0 * n_out}
+    for name, b in per_launch_bytes.items():
+        kk = kernels[name]
+        if kk["launches"]:
+            avg = kk["ms_total"] / kk["launches"]
+            kk["alg_bytes_per_launch"] = b
+            kk["hbm_frac"] = b / (avg * 1e-3) / 1e9 / peak
     dom = max(cands, key=lambda k: kernels[k]["ms_total"])
     desc, alg_bytes, tkey = cands[dom]
     avg_ms = kernels[dom]["ms_total"] / max(kernels[dom]["launches"], 1)

@@ -412,9 +412,9 @@ LNT_API int lnt_dense_lattice_mult_split(const double* A, const double* B, doubl
  * coprime integers <= 256 as INT8 tensor-core GEMMs (tcgen05) with INT32
  * accumulation, each product reduced modulo its modulus in the GEMM's
  * epilogue, and reconstructed by Chinese remaindering in exact integers;
- * beta = min(floor((log2 prod(moduli) - log2 w - 3) / 2), 53), error about
+ * beta = min(floor((log2 prod(moduli) - log2 w - 3) / 2), 52), error about
  * 2^(2-beta) |A||B| per entry (13 moduli: beta = 42 at w = 16384; 16 moduli:
- * beta = 53).  Requires w < 2^17 and 2 <= moduli <= 20. */
+ * beta = 52).  Requires w < 2^17 and 2 <= moduli <= 20. */
 LNT_API int lnt_dense_crt_workspace(int64_t h, int64_t w, int64_t wB, int moduli, size_t* bytes);
 /* The number of moduli for _crt that keeps every entry's error within
  * tol * (|A||B|)_ij (tol = 1e-12 for float64-class results): the error grows

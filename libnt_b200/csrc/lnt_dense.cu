@@ -351,19 +351,19 @@ __device__ __forceinline__ double scale2(double x, int e) {
   return (x * pow2(e1)) * pow2(e - e1);
 }
 
-// A residue of the integer-valued double x (|x| < 2^56) modulo m_l in
-// [-128, 127]: q = x / m rounded to nearest by adding 1.5 * 2^52 (exact
-// integer spacing), r = x - q m exact by fma, |r| <= m/2 + 1 (q may be one off
-// next to a half); the low word of r + 1.5 * 2^52 is r as an int.  Any
-// representative congruent modulo m serves the modular products.
+// A residue of the integer-valued double x (|x| <= 2^51, i.e. beta <= 52)
+// modulo m_l, as a byte: q = x / m rounded to nearest by adding 1.5 * 2^52
+// (exact integer spacing), r = x - q m exact by fma, and the low word of
+// r + 1.5 * 2^52 is r as an int.  1/m rounded to double errs by 2^-53
+// relatively, so x / m is off by at most 1/(4m) and |r| <= m/2 + 1/4: for odd
+// m <= 255 that is |r| <= 127, for m = 256 |r| <= 128, and the byte of 128 is
+// -128, congruent modulo 256.  Every modulus's byte is therefore an int8
+// congruent to x, which is all the modular products need.
 __device__ __forceinline__ int sym_res(double x, int l, const CrtParams& P) {
   constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
   const double q = fma(x, P.rinv_hi[l], kRound) - kRound;
   const double r = fma(-q, P.md[l], x);
-  int ri = __double2loint(r + kRound);
-  if (ri > 127) ri -= P.m[l];
-  if (ri < -128) ri += P.m[l];
-  return ri;
+  return __double2loint(r + kRound);
 }
 
 // Per-row maximum exponent of A (col-major) over a chunk of columns; eA must
@@ -389,10 +389,9 @@ __global__ void fill_int_kernel(int* __restrict__ p, u64 n, int v) {
 
 // Four residues (of four consecutive K entries) packed into one 32-bit word.
 __device__ __forceinline__ u32 pack_res4(const double (&x)[4], int l, const CrtParams& P) {
-  u32 v = 0;
-#pragma unroll
-  for (int c = 0; c < 4; ++c) v |= ((u32)sym_res(x[c], l, P) & 0xffu) << (8 * c);
-  return v;
+  const u32 lo = __byte_perm((u32)sym_res(x[0], l, P), (u32)sym_res(x[1], l, P), 0x0040);
+  const u32 hi = __byte_perm((u32)sym_res(x[2], l, P), (u32)sym_res(x[3], l, P), 0x0040);
+  return __byte_perm(lo, hi, 0x5410);  // bytes x0, x1, x2, x3
 }
 
 // A (h x w col-major) -> residues res[l]: Mp rows of Kp int8 (row-major, K
@@ -463,6 +462,8 @@ __global__ void residue_b_kernel(const double* __restrict__ B, u64 w, u64 wB, u6
 // over columns.  (Unrolling the modulus loop to its compile-time bound, so
 // that the moduli tables become direct constant operands, measured slower at
 // 13 moduli: 5.35 against 4.69 ms at 16384^2.)
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 template <int LV>
 __global__ void __launch_bounds__(256) crt_kernel(const unsigned char* __restrict__ res, u64 Mp, u64 Np, u64 h,
                                                   u64 wB, CrtParams P, const int* __restrict__ eA,
@@ -475,13 +476,25 @@ __global__ void __launch_bounds__(256) crt_kernel(const unsigned char* __restric
   for (int c = 0; c < 4; ++c) ea[c] = i0 + c < h ? eA[i0 + c] - 2 * P.beta : 0;
   constexpr long long kMask = (1ll << kLimbBits) - 1;
   constexpr double kRadix = (double)(1ll << kLimbBits);
+  const u64 w0 = i0 - 4 * (threadIdx.x & 31);  // the warp's first row: 128 rows, <= 128 bytes per plane
   for (u64 j = blockIdx.y; j < wB; j += gridDim.y) {
+    // the next column's residue lines (one or two per plane) into L1 while
+    // this column accumulates: the loads below otherwise wait on DRAM
+    const u64 jn = j + gridDim.y;
+    if (jn < wB) {
+      for (int t = threadIdx.x & 31; t < 2 * P.n; t += 32) {
+        const u64 r = (t & 1) && w0 + 127 < Mp ? w0 + 127 : w0;
+        prefetch_l1(res + (u64)(t >> 1) * plane + r + Mp * jn);
+      }
+    }
     long long acc[4][LV + 1];
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
       for (int b = 0; b <= LV; ++b) acc[c][b] = 0;
     const unsigned char* src = res + i0 + Mp * j;
+    // (loading four moduli's words before using any measured slower: 72
+    // registers instead of 60 cost a quarter of the resident warps)
 #pragma unroll 2
     for (int l = 0; l < P.n; ++l) {
       const u32 w4 = __ldcs(reinterpret_cast<const u32*>(src + (u64)l * plane));
@@ -614,7 +627,9 @@ int make_crt_params(int n, u64 K, CrtParams* P) {
   }
   const int beta = (int)std::floor((log2M - std::log2((double)K) - 3.0) / 2.0);
   if (beta < 8) return LNT_UNSUPPORTED;
-  P->beta = std::min(beta, 53);  // |A'|, |B'| < 2^52: exact doubles, and residues by 1.5 * 2^52 rounding
+  // |A'|, |B'| <= 2^51: exact doubles, and symmetric residues that fit int8
+  // without a range correction (sym_res)
+  P->beta = std::min(beta, 52);
   for (int l = 0; l < n; ++l) {
     const int m = P->m[l];
     long long rest = 1;  // (M / m) mod m
@@ -798,7 +813,7 @@ int lnt_dense_crt_moduli(const double* A, const double* B, int64_t h, int64_t w,
   const int need_beta = (int)std::ceil(2.0 + lr - std::log2(tol));
   for (int n = 2; n <= kMaxModuli; ++n) {
     CrtParams P;
-    if (make_crt_params(n, (u64)w, &P) == LNT_OK && P.beta >= std::min(need_beta, 53)) {
+    if (make_crt_params(n, (u64)w, &P) == LNT_OK && P.beta >= std::min(need_beta, 52)) {
       *moduli = n;
       return LNT_OK;
     }
