@@ -824,7 +824,7 @@ def run_batched(args):
     import oracle
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", torch.cuda.current_device())
-    dims, tdims, a_off, b_off, ak, av, bk, bv = batched_inputs(seed=rank)
+    dims, tdims, a_off, b_off, ak, av, bk, bv = batched_inputs(count=args.batch_count, seed=rank)
     count = len(dims)
     cat = [np.concatenate(x) for x in (ak, av, bk, bv)]
     dt = [torch.from_numpy(x.view(np.int64) if x.dtype == np.uint64 else x).to(dev) for x in cat]
@@ -890,7 +890,7 @@ def run_batched(args):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     lp = 0
-    for p in range(count):
+    for p in range(0 if args.no_loop else count):
         a0, a1, b0, b1 = int(a_off[p]), int(a_off[p + 1]), int(b_off[p]), int(b_off[p + 1])
         h, w, wB, _ = (int(x) for x in dims[p])
         ka, va = L.permute_sort(dt[0][a0:a1], dt[1][a0:a1], max_key=h * w)
@@ -921,7 +921,7 @@ def run_batched(args):
             cp += int(cnt[batched_b_rows(bk[p], tdims[p][1])].sum())
         t = time.perf_counter() - t0
         cpu = {"value": cp / t, "unit": "products/s", "cores": 1, "kind": kind,
-               "sample": f"first {n_cpu} of the 4096 problems from the same unsorted tensors: "
+               "sample": f"first {n_cpu} of the {count} problems from the same unsorted tensors: "
                          + ("the reference's radix sort of a, its re-key and radix sort of b"
                             if kind == "reference" else "restated sorts")
                          + ", restated csc_no_accum, one thread"}
@@ -930,7 +930,7 @@ def run_batched(args):
     peak, peak_kind = peaks()
     avg = os_ms / max(os_n, 1)
     achieved = 32.0 * n_pairs / (avg * 1e-3) / 1e9 if os_n else 0.0
-    config = {"workload": "4096 independent sparse contractions c(i,l)=a(i,j,k)*b(k,l,j): dims U{16..512}, nnz "
+    config = {"workload": f"{count} independent sparse contractions c(i,l)=a(i,j,k)*b(k,l,j): dims U{{16..512}}, nnz "
                           "log-U[1e2,1e5] per operand, f64 U[-1,1], both operands unsorted tensors; a step = one "
                           "CUDA-graph replay of lnt_batched_contract (re-key, one segmented radix sort of all "
                           "operands, persistent SPA products)",
@@ -938,9 +938,10 @@ def run_batched(args):
               "queue_chunk": os.environ.get("LNT_BATCH_CHUNK") or tuned_value("batch_chunk"),
               "l2": "operands (1.9 GB) larger than the 126 MB L2"}
     print(json.dumps(_line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
-        "per_contraction_loop": {"problems": count, "ms": loop_s * 1e3, "products_per_s": lp / loop_s,
-                                 "note": "per problem: lnt_permute_sort of a, of b with its re-key, "
-                                         "lnt_lattice_mult_plan + count read-back + lnt_lattice_mult"},
+        "per_contraction_loop": None if args.no_loop else {
+            "problems": count, "ms": loop_s * 1e3, "products_per_s": lp / loop_s,
+            "note": "per problem: lnt_permute_sort of a, of b with its re-key, "
+                    "lnt_lattice_mult_plan + count read-back + lnt_lattice_mult"},
         "oracle_check": {"problems": checked, "ok": True},
         "kernels": kernels,
         "gpu_launches": launches, "cpu_baseline": cpu, "clocks": sampler.summary(),
@@ -1610,6 +1611,8 @@ def main():
     ap.add_argument("--moduli", type=int, default=13, help="dense scheme II: moduli (uniform data)")
     ap.add_argument("--no-scheme1", action="store_true", help="dense: skip timing scheme I")
     ap.add_argument("--dense-log2", type=int, default=14, help="dense: log2 of the GEMM size (14 = the workload)")
+    ap.add_argument("--batch-count", type=int, default=4096, help="batched: problems (4096 = the workload)")
+    ap.add_argument("--no-loop", action="store_true", help="batched: skip the per-contraction loop (profiling)")
     ap.add_argument("--skew-log2", type=int, default=25, help="skewed: log2 of coordinates drawn per operand")
     ap.add_argument("--shrink", type=int, default=0, help="outer / unary: divide the workload by 2^shrink (profiling)")
     ap.add_argument("--skew-b-log2", type=int, default=None, help="skewed: log2 of coordinates drawn for b "
