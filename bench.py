@@ -1021,6 +1021,27 @@ def measure_dense(args):
                 for k in ("dense_residues", "dense_exp_a", "dense_exp_b", "dense_residue_a", "dense_residue_b",
                           "dense_mod_gemm", "dense_crt")}
         L.profile_reset()
+        e2e = None
+        if variant == "uniform" and not args.no_e2e:
+            # the public call on operands copied from pinned host memory every
+            # step, the product copied back
+            hA, hB = A.cpu().pin_memory(), B.cpu().pin_memory()
+            hC = torch.empty(n * n, dtype=torch.float64, pin_memory=True)
+            dA, dB = torch.empty_like(A), torch.empty_like(B)
+
+            def e2e_step():
+                dA.copy_(hA, non_blocking=True)
+                dB.copy_(hB, non_blocking=True)
+                L.dense_mult_crt(dA, dB, n, n, n, 1, moduli, out=Cc, ws=wsc)
+                hC.copy_(Cc, non_blocking=True)
+            t_e2e = timed(e2e_step)
+            if not torch.equal(hC, Cc.cpu()):
+                raise RuntimeError("dense end-to-end product differs from the device-resident one")
+            e2e = {"value": flops / (t_e2e * 1e-3) / 1e12, "unit": "TFLOP/s (FP64-equivalent)", "ms_per_step": t_e2e,
+                   "h2d_bytes_per_step": 2 * 8 * n * n, "d2h_bytes_per_step": 8 * n * n,
+                   "note": "lnt_dense_lattice_mult_crt on A and B copied from pinned host memory every step, "
+                           "C copied back; one stream"}
+            del hA, hB, hC, dA, dB
         del wsc
         torch.cuda.empty_cache()
         Ah, Bh = A.cpu().numpy(), B.cpu().numpy()
@@ -1041,7 +1062,7 @@ def measure_dense(args):
                "max_diff_vs_fp64_over_maxC": full, "sampled_entries": int(rows.size),
                "kernels_ms_per_step": kern,
                "int8_tensor_tops": moduli * 2.0 * n ** 3 / (kern["dense_mod_gemm"] * 1e-3) / 1e12,
-               "clocks": sampler.summary()}
+               "clocks": sampler.summary(), "e2e": e2e}
         if not args.no_scheme1:
             wss = L.workspace(L.dense_split_workspace(n, n, n, slices), dev)
             t_split = timed(lambda: L.dense_mult_split(A, B, n, n, n, 1, slices, out=Cc, ws=wss))
@@ -1067,6 +1088,31 @@ def measure_dense(args):
     e1.record()
     torch.cuda.synchronize()
     int8_peak = 2 * 8192 ** 3 / (e0.elapsed_time(e1) / 10 * 1e-3) / 1e12
+    cpu = None
+    if not args.no_cpu:
+        # the reference's GEMM is Eigen 3.2.5, which is not in the image: numpy's
+        # float64 matmul on the host's BLAS stands in, on a bounded sample
+        m = 4096
+        hr = np.random.default_rng(3)
+        Ah = hr.uniform(-1, 1, (m, m))
+        Bh = hr.uniform(-1, 1, (m, m))
+        Ah @ Bh
+        best = float("inf")
+        for _ in range(3):
+            t0 = time.perf_counter()
+            Ah @ Bh
+            best = min(best, time.perf_counter() - t0)
+        threads, blas = os.cpu_count(), "BLAS"
+        try:
+            from threadpoolctl import threadpool_info
+            info = [i for i in threadpool_info() if i.get("user_api") == "blas"]
+            if info:
+                threads, blas = int(info[0].get("num_threads", threads)), str(info[0].get("internal_api", "BLAS"))
+        except Exception:
+            pass
+        cpu = {"value": 2.0 * m ** 3 / best / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+               "sample": f"numpy float64 matmul {m}^3 on the host's {blas} ({threads} threads), a labelled stand-in "
+                         "for the reference's Eigen GEMM (not in the image); best of 3"}
     u = results["uniform"]
     config = {"workload": f"dense contraction c(i,j,m,n)=a(i,j,k,l)*b(k,l,m,n), dims 128 (a {n}^3 FP64 GEMM); "
                           "Ozaki scheme II: beta-bit integer operands, 13 (U[-1,1]) / 16 (2^+-20 exponents) moduli "
@@ -1079,7 +1125,7 @@ def measure_dense(args):
                                                   "reduced modulo m in the epilogue)", "achieved": u["int8_tensor_tops"],
                      "peak": int8_peak, "unit": "TOP/s", "frac": u["int8_tensor_tops"] / int8_peak,
                      "peak_source": "int8 torch._int_mm 8192^3 measured in this run (MEASURED_PEAKS.json has bf16 only)"},
-        "vs_fp64_gemm": u["speedup_vs_fp64"], "clocks": u["clocks"],
+        "vs_fp64_gemm": u["speedup_vs_fp64"], "clocks": u["clocks"], "cpu_baseline": cpu, "e2e": u["e2e"],
     })
 
 def _timed_steps(torch, step, args):
