@@ -2,10 +2,10 @@
 // wide keys and many pairs (the sparse merge under permutation):
 //
 //   1. bucket_hist_kernel: one read of all (re-keyed, concatenated) keys
-//      counts the 2^T buckets given by the top T key bits (T <= 15; one CTA
-//      per SM with the whole histogram in shared memory); the last CTA derives
-//      the bucket starts, the maximum bucket size and the digit histograms of
-//      the two passes below.
+//      counts the 2^T buckets given by the top T key bits (T <= 15; 16-bit
+//      counts in shared memory, two CTAs per SM); the last CTA derives the
+//      bucket starts, the maximum bucket size and the digit histograms of the
+//      two passes below.
 //   2. two stable one-sweep passes on the top T bits (T-8 bits, then 8 bits)
 //      group the pairs by bucket; the first reads through the PairSource
 //      (re-key + concatenation fused);
@@ -528,11 +528,15 @@ bool small_geometry() {
   return kTunedBucketSmall != 0;
 }
 
+// Bucket bits for n pairs: ceil(log2 n) - 12 (large geometry), so that the
+// average bucket holds between 2048 and 4096 pairs, below the CTA capacity
+// (5120); rounding log2 n down would put n = 3 x 2^25 at 6144 per bucket and
+// send every such call to the LSD path.
 int bucket_bits_for(u32 n, bool small) {
   int lg = 0;
-  while ((1u << (lg + 1)) <= n && lg < 31) ++lg;
-  return small ? std::max(9, std::min(16, lg - 11))   // about 2048 pairs per bucket
-               : std::max(9, std::min(15, lg - 12));  // about 4096 pairs per bucket
+  while (lg < 31 && (1u << lg) < n) ++lg;  // ceil(log2 n)
+  return small ? std::max(9, std::min(16, lg - 11))   // 1024..2048 pairs per bucket
+               : std::max(9, std::min(15, lg - 12));  // 2048..4096 pairs per bucket
 }
 
 struct BucketLayout {
