@@ -258,36 +258,74 @@ __global__ void tile_cbits_kernel(const u64* __restrict__ ak, const u64* __restr
   }
 }
 
-// cnt[(t*wB + col)*np + p] = pattern bits of column col among panel p's rows;
-// warp per (t, p, bitmap word q).
+__device__ __forceinline__ u64 shfl_xor64(u64 v, int o) {
+  const u32 lo = __shfl_xor_sync(FULL, (u32)v, o), hi = __shfl_xor_sync(FULL, (u32)(v >> 32), o);
+  return ((u64)hi << 32) | lo;
+}
+
+// The warp's 32 x 64 bit matrix (one 64-bit word per lane) as six bit
+// slices of its 64 column counts (each <= 32), held by every lane.  Bit-sliced
+// butterfly: s[i] holds bit i of the counts; the step with offset o adds the
+// partner lane's counts with a ripple carry over the slices, so after five
+// steps every lane holds the counts of all 32 lanes (30 shuffles and about 75
+// logic operations instead of 128 ballots and population counts).
+__device__ __forceinline__ void column_count_slices(u64 word, u64 (&s)[6]) {
+  s[0] = word;
+#pragma unroll
+  for (int step = 0; step < 5; ++step) {
+    const int o = 1 << step;
+    u64 c = 0;
+#pragma unroll
+    for (int i = 0; i <= step; ++i) {  // step + 1 slices before this step
+      const u64 a = s[i], b = shfl_xor64(a, o);
+      s[i] = a ^ b ^ c;
+      c = (a & b) | (c & (a ^ b));
+    }
+    s[step + 1] = c;
+  }
+}
+
+// cnt[(t*wB + col)*np + p] = pattern bits of column col among panel p's rows.
+// Warp per (t, group of 32 panels, bitmap word q): for each panel of the
+// group the lanes (one row each) form the column counts of its 64 columns,
+// and lane i keeps panel i's slices (12 registers); then, column by column,
+// the 32 lanes write the group's 32 consecutive counts as one 128-byte store.
+// (One warp per panel wrote 64 counts 4 bytes at a time, np words apart.)
+static_assert(kPanelRows == 32, "tile_count_kernel takes a panel as one row per lane");
 __global__ void tile_count_kernel(const u64* __restrict__ cbits, u64 h, u64 wB, u64 d, u32 nt, u32 np,
                                   u32* __restrict__ cnt) {
   // here nt counts bitmap words per row
   const int lane = threadIdx.x & 31;
-  const u64 units = d * np * (u64)nt;
-  const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
-  for (u64 u = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < units; u += nw) {
-    const u64 t = u / ((u64)np * nt);
-    const u64 rem = u - t * np * nt;
-    const u32 p = (u32)(rem / nt);
-    const u32 q = (u32)(rem - (u64)p * nt);
-    u32 clo = 0, chi = 0;
-    for (int g = 0; g < kPanelRows / 32; ++g) {
-      const u64 r = (u64)p * kPanelRows + g * 32 + lane;
+  const u32 ng = (np + 31) / 32;
+  const u64 units = d * (u64)ng * nt;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 u = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < units; u += nwarps) {
+    const u64 t = u / ((u64)ng * nt);
+    const u64 rem = u - t * ng * nt;
+    const u32 g = (u32)(rem / nt);
+    const u32 q = (u32)(rem - (u64)g * nt);
+    u64 keep[6] = {0, 0, 0, 0, 0, 0};
+    for (int pp = 0; pp < 32; ++pp) {
+      const u32 p = g * 32 + pp;
+      if (p >= np) break;  // uniform across the warp
+      const u64 r = (u64)p * kPanelRows + lane;  // a panel is one row per lane
       const u64 word = r < h ? cbits[(r + h * t) * nt + q] : 0ull;
+      u64 sl[6];
+      column_count_slices(word, sl);
+      if (lane == pp) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const u32 lo = __popc(__ballot_sync(FULL, (word >> j) & 1ull));
-        const u32 hi = __popc(__ballot_sync(FULL, (word >> (32 + j)) & 1ull));
-        if (lane == j) {
-          clo += lo;
-          chi += hi;
-        }
+        for (int i = 0; i < 6; ++i) keep[i] = sl[i];
       }
     }
-    const u64 c0 = (u64)q * kWordCols + lane, c1 = c0 + 32;
-    if (c0 < wB) cnt[(t * wB + c0) * np + p] = clo;
-    if (c1 < wB) cnt[(t * wB + c1) * np + p] = chi;
+    const u32 p = g * 32 + lane;
+    for (int c = 0; c < kWordCols; ++c) {
+      const u64 col = (u64)q * kWordCols + c;
+      if (col >= wB) break;
+      u32 v = 0;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) v |= (u32)((keep[i] >> c) & 1ull) << i;
+      if (p < np) cnt[(t * wB + col) * np + p] = v;
+    }
   }
 }
 
@@ -578,7 +616,8 @@ int run_tile_mult(const u64* akeys, const double* avals, u64 na, const u64* bkey
   }
   {
     ProfScope prof("tile_count", s);
-    tile_count_kernel<<<grid_cap(d * t.np * (u64)t.nw * 32, 256), 256, 0, s>>>(cbits, h, wB, d, t.nw, t.np, cnt);
+    tile_count_kernel<<<grid_cap(d * ((t.np + 31) / 32) * (u64)t.nw * 32, 256), 256, 0, s>>>(cbits, h, wB, d, t.nw,
+                                                                                              t.np, cnt);
     count_launch();
   }
   if ((st = scan::run(CountGet{cnt}, ncnt, base, (unsigned long long*)d_nc, at(L.scan), s, "tile_scan")) != LNT_OK)
