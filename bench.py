@@ -526,7 +526,7 @@ def run_ours(args):
     peak, peak_kind = peaks()
     prof_file = "onesweep8_bucket_merge_512x4_2x64M"
     cands = {
-        "sort_onesweep": ("one 8-bit digit pass of the bucketed sort over 2^27 (u64,f64) pairs", 32.0 * n,
+        "sort_onesweep": ("one digit pass (7 then 8 bits) of the bucketed sort over 2^27 (u64,f64) pairs", 32.0 * n,
                           "traffic_bytes_per_pair"),
         "bucket_sort_collect": ("per-bucket shared-memory sort + duplicate fold of the 2^27 pairs",
                                 16.0 * n + 16.0 * n_out, "bucket_traffic_bytes_per_pair"),
@@ -559,8 +559,10 @@ def run_ours(args):
         torch.cuda.empty_cache()
         sub = argparse.Namespace(**vars(args))
         sub.steps, sub.warmup, sub.no_scheme1 = min(args.steps, 5), 3, True
-        for key, fn in (("skewed_contraction", measure_skewed), ("dense", measure_dense)):
-            d = fn(sub)
+        for key, fn in (("skewed_contraction", measure_skewed), ("dense", measure_dense),
+                        ("batched", measure_batched), ("contraction", measure_contraction)):
+            # (the 0.1 ms contraction replay keeps the full step count)
+            d = fn(argparse.Namespace(**{**vars(sub), "steps": args.steps}) if key == "contraction" else sub)
             torch.cuda.empty_cache()
             if d is not None:
                 extra[key] = {k: v for k, v in d.items() if k not in ("metric", "n_gpus", "scaling", "vs_baseline", "data")}
@@ -626,7 +628,7 @@ def contraction_inputs(seed=0):
     return ak, rng.uniform(-1, 1, 10 ** 4), bk, rng.uniform(-1, 1, 10 ** 4)
 
 
-def run_contraction(args):
+def measure_contraction(args):
     """Plain sparse contraction, MIA level: toStraightLattice(a) (sort), toLatticeSort(b)
     (re-key to {2,0,1} + sort), csc_no_accum, all through the C ABI."""
     import torch
@@ -738,7 +740,7 @@ def run_contraction(args):
     ms = graph_ms["ms"]
     e2e_ms = e2e_graph_ms["ms"]
     if rank != 0:
-        return 0
+        return None
     cpu = None
     if not args.no_cpu:
         import oracle
@@ -763,12 +765,18 @@ def run_contraction(args):
                           "replay of that sequence of C-ABI calls",
               "products": prods, "output_nnz": nc, "l2": "inputs fit in L2 (latency-bound workload)",
               "eager_ms_per_step": eager_ms, "eager_e2e_ms_per_step": e2e_eager_ms}
-    print(json.dumps(_line("products/s", prods * world / (ms * 1e-3), ms, args, world, config, {
+    return _line("products/s", prods * world / (ms * 1e-3), ms, args, world, config, {
         "e2e": {"value": prods * world / (e2e_ms * 1e-3), "unit": "products/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 4 * 8 * 10 ** 4, "d2h_bytes_per_step": 16 * nc + 16},
         "gpu_launches": launches, "cpu_baseline": cpu,
         "roofline": {"bound": "latency", "note": "about 0.5 MB of data: the step is launch- and latency-bound"},
-    })), flush=True)
+    })
+
+
+def run_contraction(args):
+    d = measure_contraction(args)
+    if d is not None:
+        print(json.dumps(d), flush=True)
     return 0
 
 
@@ -817,7 +825,7 @@ def batched_expected(p, dims, tdims, ak, av, bk, bv, with_abs=False):
     return oracle.lattice_mult(ak[p][oa], av[p][oa], h, w, 1, kb[ob], bv[p][ob], wB, with_abs=with_abs)
 
 
-def run_batched(args):
+def measure_batched(args):
     import torch
 
     import libnt_b200 as L
@@ -900,7 +908,7 @@ def run_batched(args):
     torch.cuda.synchronize()
     loop_s = time.perf_counter() - t0
     if rank != 0:
-        return 0
+        return None
     cpu = None
     if not args.no_cpu:
         n_cpu = 256
@@ -937,7 +945,7 @@ def run_batched(args):
               "problems": count, "pairs_sorted": n_pairs, "products": products, "output_nnz": out_total,
               "queue_chunk": os.environ.get("LNT_BATCH_CHUNK") or tuned_value("batch_chunk"),
               "l2": "operands (1.9 GB) larger than the 126 MB L2"}
-    print(json.dumps(_line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
+    return _line("products/s", products * world / (ms * 1e-3), ms, args, world, config, {
         "per_contraction_loop": None if args.no_loop else {
             "problems": count, "ms": loop_s * 1e3, "products_per_s": lp / loop_s,
             "note": "per problem: lnt_permute_sort of a, of b with its re-key, "
@@ -949,7 +957,13 @@ def run_batched(args):
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "alg_bytes_per_launch": 32.0 * n_pairs, "avg_launch_ms": avg,
                      "traffic": None},
-    })), flush=True)
+    })
+
+
+def run_batched(args):
+    d = measure_batched(args)
+    if d is not None:
+        print(json.dumps(d), flush=True)
     return 0
 
 
@@ -1649,7 +1663,7 @@ def main():
                     help="log2 of non-zeros per operand (26 = the workload; smaller only for profiling)")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--no-extra", action="store_true",
-                    help="merge line only: skip the skewed-contraction and dense keys")
+                    help="merge line only: skip the skewed-contraction, dense, batched and contraction keys")
     ap.add_argument("--workload", default="merge", choices=["merge", "contraction", "batched", "dense", "skewed", "outer", "unary", "scanmerge", "mixed"],
                     help="merge (default: the sparse merge under permutation), contraction (100^3 plain "
                          "contraction), batched (4096 uneven contractions), dense (128^4 dense contraction)")
