@@ -1028,8 +1028,10 @@ def measure_dense(args):
         L.profile_reset()
         L.profile_enable(True)
         sampler = ClockSampler(torch.cuda.current_device())
+        c0 = L.launch_count()
         with sampler:
             t_crt = timed(lambda: L.dense_mult_crt(A, B, n, n, n, 1, moduli, out=Cc, ws=wsc))
+        per_call = (L.launch_count() - c0) // (reps + max(1, args.warmup // 3))
         L.profile_enable(False)
         kern = {k: L.profile_query(k)[0] / (reps + max(1, args.warmup // 3))
                 for k in ("dense_residues", "dense_exp_a", "dense_exp_b", "dense_residue_a", "dense_residue_b",
@@ -1076,7 +1078,7 @@ def measure_dense(args):
                "max_diff_vs_fp64_over_maxC": full, "sampled_entries": int(rows.size),
                "kernels_ms_per_step": kern,
                "int8_tensor_tops": moduli * 2.0 * n ** 3 / (kern["dense_mod_gemm"] * 1e-3) / 1e12,
-               "clocks": sampler.summary(), "e2e": e2e}
+               "clocks": sampler.summary(), "e2e": e2e, "gpu_launches": per_call * reps}
         if not args.no_scheme1:
             wss = L.workspace(L.dense_split_workspace(n, n, n, slices), dev)
             t_split = timed(lambda: L.dense_mult_split(A, B, n, n, n, 1, slices, out=Cc, ws=wss))
@@ -1140,6 +1142,7 @@ def measure_dense(args):
                      "peak": int8_peak, "unit": "TOP/s", "frac": u["int8_tensor_tops"] / int8_peak,
                      "peak_source": "int8 torch._int_mm 8192^3 measured in this run (MEASURED_PEAKS.json has bf16 only)"},
         "vs_fp64_gemm": u["speedup_vs_fp64"], "clocks": u["clocks"], "cpu_baseline": cpu, "e2e": u["e2e"],
+        "gpu_launches": u["gpu_launches"],
     })
 
 def _timed_steps(torch, step, args):
