@@ -231,8 +231,11 @@ __global__ void tile_bentry_kernel(const u64* __restrict__ bk, const double* __r
 }
 
 // Cbits[row] = OR of Bbits[c + w*t] over the A entries (row, c); warp per row.
+// A warp stops reading B rows once every lane's word is full (all wB columns
+// of its 64 set): further rows cannot change it, and rows of the hottest B
+// entries are full under skewed inputs.
 __global__ void tile_cbits_kernel(const u64* __restrict__ ak, const u64* __restrict__ arow,
-                                  const u64* __restrict__ bbits, u64 h, u64 w, u64 d, u32 nw, Divider div_h,
+                                  const u64* __restrict__ bbits, u64 h, u64 w, u64 d, u32 nw, u64 wB, Divider div_h,
                                   u64* __restrict__ cbits) {
   const int lane = threadIdx.x & 31;
   const u64 nrows = h * d;
@@ -243,14 +246,21 @@ __global__ void tile_cbits_kernel(const u64* __restrict__ ak, const u64* __restr
     const u64 cbase = w * t - w * row;  // B row = A key + cbase
     for (u32 w0 = 0; w0 < nw; w0 += 32) {
       const u32 word = w0 + lane;
+      const u64 rest = wB - (u64)word * kWordCols;  // columns of this word
+      const u64 full = word >= nw ? 0ull : rest >= 64 ? ~0ull : (1ull << rest) - 1ull;
       u64 acc = 0;
-      for (u64 eb = e0; eb < e1; eb += 32) {
+      bool done = word >= nw;
+      for (u64 eb = e0; eb < e1 && !__all_sync(FULL, done); eb += 32) {
         const u64 e = eb + lane;
         const u64 br = e < e1 ? ak[e] + cbase : 0;
         const int n = (int)(e1 - eb < 32 ? e1 - eb : 32);
         for (int k = 0; k < n; ++k) {
           const u64 b = __shfl_sync(FULL, br, k);
-          if (word < nw) acc |= bbits[b * nw + word];
+          if (!done) {
+            acc |= bbits[b * nw + word];
+            done = acc == full;
+          }
+          if (__all_sync(FULL, done)) break;
         }
       }
       if (word < nw) cbits[row * nw + word] = acc;
@@ -610,8 +620,8 @@ int run_tile_mult(const u64* akeys, const double* avals, u64 na, const u64* bkey
   }
   {
     ProfScope prof("tile_cbits", s);
-    tile_cbits_kernel<<<grid_cap(crows * 32, 256), 256, 0, s>>>(ak, arow, bbits, h, w, d, t.nw, make_divider(h),
-                                                               cbits);
+    tile_cbits_kernel<<<grid_cap(crows * 32, 256), 256, 0, s>>>(ak, arow, bbits, h, w, d, t.nw, wB,
+                                                               make_divider(h), cbits);
     count_launch();
   }
   {
