@@ -326,7 +326,7 @@ LNT_API int lnt_contract_attract(const uint64_t* keys, const double* vals, size_
 /* ---- batched lattice products ------------------------------------------- */
 
 /* `count` independent products C_p = A_p * B_p, each as lnt_lattice_mult
- * (rows beyond 1024 are accumulated in blocks of 1024).  Host arrays: dims_host[4p..4p+3] =
+ * (rows beyond 512 are accumulated in blocks of 512).  Host arrays: dims_host[4p..4p+3] =
  * (rows(A_p), cols(A_p) = rows(B_p), cols(B_p), tabs); a_off_host / b_off_host
  * (count+1 entries) delimit each problem's operand inside the concatenated
  * device arrays a_keys/a_vals, b_keys/b_vals (each lattice key-sorted).

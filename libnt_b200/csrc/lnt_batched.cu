@@ -19,8 +19,8 @@
 //   coff: per-problem output offsets.
 // The queue chunk size (units per grab) is the segment-split knob the
 // autotuner sets: small chunks balance uneven columns, large ones cut queue
-// traffic.  Problems with more than 1024 rows are accumulated in blocks of
-// 1024 rows (each A column's entries for the block found by binary search).
+// traffic.  Problems with more than 512 rows are accumulated in blocks of
+// 512 rows (each A column's entries for the block found by binary search).
 //
 // lnt_batched_contract takes the operands as the tensors are stored (unsorted,
 // keys in each tensor's own mode order) and does the per-problem work of
@@ -42,7 +42,7 @@
 namespace lnt {
 namespace {
 
-constexpr int kMaxRows = 1024;  // accumulator rows per warp
+constexpr int kMaxRows = 512;  // accumulator rows per warp (4 KB of FP64 sums: eight 4-warp CTAs per SM)
 constexpr int kWarps = 4;
 
 struct ProbDesc {
@@ -199,7 +199,31 @@ __global__ void __launch_bounds__(kWarps * 32) batch_spa_kernel(BatchArgs args, 
           const u32 hi = aptr[acol + 1];
           if (blocked) lo = lower_row(ak, kmask, lo, hi, abase, r0);
           const double beta = NUMERIC ? bv[e] : 0.0;
-          for (u32 x = lo; x < hi; ++x) {
+          // four A entries loaded before their accumulations, so that their
+          // loads overlap instead of each waiting behind the previous atomics
+          bool stop = false;
+          u32 x = lo;
+          for (; x + 4 <= hi && !stop; x += 4) {
+            u64 kk[4];
+            double vv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              kk[j] = ak[x + j];
+              vv[j] = NUMERIC ? av[x + j] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const u64 rr = (kk[j] & kmask) - abase;
+              if (blocked && rr >= r0 + hb) {
+                stop = true;
+                break;
+              }
+              const u32 r = (u32)(rr - r0);
+              atomicOr(&bits[r >> 5], 1u << (r & 31));
+              if (NUMERIC) atomicAdd(&acc[r], vv[j] * beta);
+            }
+          }
+          for (; x < hi && !stop; ++x) {
             const u64 rr = (ak[x] & kmask) - abase;
             if (blocked && rr >= r0 + hb) break;
             const u32 r = (u32)(rr - r0);
@@ -419,15 +443,22 @@ int run_batch_product(const BatchArgs& args, const BatchLayout& L, unsigned char
   const u32 chunk = batch_chunk();
   {
     ProfScope prof("batch_spa_symbolic", s);
-    batch_spa_kernel<false><<<sms * 8, kWarps * 32, 0, s>>>(args, chunk, queue, ucount, nullptr, nullptr, nullptr);
+    int per_sm = 0;  // persistent: as many CTAs as fit
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_spa_kernel<false>, kWarps * 32, 0) != cudaSuccess)
+      return LNT_DEVICE_ERROR;
+    batch_spa_kernel<false><<<sms * std::max(per_sm, 1), kWarps * 32, 0, s>>>(args, chunk, queue, ucount, nullptr,
+                                                                              nullptr, nullptr);
     count_launch();
   }
   st = scan::run(U64Of{ucount}, L.total_units, (unsigned long long*)uoff, nullptr, w + L.off_scan, s, "batch_scan");
   if (st != LNT_OK) return st;
   {
     ProfScope prof("batch_spa_numeric", s);
-    batch_spa_kernel<true><<<sms * 6, kWarps * 32, 0, s>>>(args, chunk, queue + 1, nullptr, uoff, (u64*)c_keys,
-                                                           c_vals);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_spa_kernel<true>, kWarps * 32, 0) != cudaSuccess)
+      return LNT_DEVICE_ERROR;
+    batch_spa_kernel<true><<<sms * std::max(per_sm, 1), kWarps * 32, 0, s>>>(args, chunk, queue + 1, nullptr, uoff,
+                                                                             (u64*)c_keys, c_vals);
     count_launch();
   }
   {
