@@ -82,12 +82,14 @@ def test_batched_cuda_graph_replay(cuda, torch, rng):
 
 
 def test_batched_rows_beyond_one_accumulator(cuda, torch, rng):
-    """Problems with more than 1024 rows are accumulated in blocks of 1024 rows
-    (a binary search per A column and block): same results as the oracle."""
+    """Problems with more than 512 rows are accumulated in blocks of 512 rows
+    (a binary search per A column and block): same results as the oracle,
+    at the block boundary (512, 513 rows) and well beyond it."""
     import libnt_b200 as L
     dims, ak, av, bk, bv = [], [], [], [], []
     for h, w, wB, na, nb in [(3000, 40, 30, 20000, 500), (1025, 8, 9, 4000, 50), (2048, 1, 3, 2048, 3),
-                             (5000, 16, 4, 0, 30), (1500, 20, 20, 6000, 0)]:
+                             (5000, 16, 4, 0, 30), (1500, 20, 20, 6000, 0), (512, 8, 9, 3000, 40),
+                             (513, 8, 9, 3000, 40)]:
         a = np.sort(rng.choice(h * w, na, replace=False)).astype(np.uint64)
         b = np.sort(rng.choice(w * wB, nb, replace=False)).astype(np.uint64)
         dims.append((h, w, wB, 1))
@@ -108,7 +110,7 @@ def test_batched_rows_beyond_one_accumulator(cuda, torch, rng):
 def _unsorted_batch(rng, count, dim_lo, dim_hi, nnz_lo, nnz_hi, tall=()):
     """Problems c(i,l) = a(j,i,k) * b(k,l,j) as unsorted tensors: a's keys run j
     fastest (re-key {1,0,2} puts i first), b's keys k fastest (re-key {2,0,1});
-    `tall` problems get i beyond the 1024-row accumulator."""
+    `tall` problems get i beyond the 512-row accumulator."""
     import libnt_b200 as L
     dims, specs_a, specs_b, ak, av, bk, bv = [], [], [], [], [], [], []
     for p in range(count):
