@@ -146,7 +146,7 @@ __device__ __forceinline__ u32 lower_row(const u64* __restrict__ ak, u64 kmask, 
 }
 
 template <bool NUMERIC>
-__global__ void __launch_bounds__(kWarps * 32) batch_spa_kernel(BatchArgs args, u32 chunk, u32* __restrict__ queue,
+__global__ void __launch_bounds__(kWarps * 32, 8) batch_spa_kernel(BatchArgs args, u32 chunk, u32* __restrict__ queue,
                                                                  u64* __restrict__ ucount,
                                                                  const u64* __restrict__ uoff,
                                                                  u64* __restrict__ ck, double* __restrict__ cv) {
