@@ -346,22 +346,29 @@ struct U64Of {
 
 // Composite sort keys of the contract path: position q of the concatenated
 // operand (A or B) belongs to the problem p with off[p] <= q < off[p+1]; its
-// key is re-keyed into p's lattice order and prefixed with (p, which).  Each
-// thread takes 8 consecutive positions (one binary search).
+// key is re-keyed into p's lattice order and prefixed with (p, which).  A warp
+// takes 256 consecutive positions, lane-striped (position base + 32 j + lane),
+// so loads and stores are coalesced; each lane finds its first position's
+// problem by binary search and walks forward from there.  (A thread taking 8
+// consecutive positions issued 8-byte stores 64 bytes apart: 0.86 ms for the
+// 4096-problem batch.)
 __global__ void batch_compose_kernel(const u64* __restrict__ keys, u64 n, const uint64_t* __restrict__ off,
                                      int count, const RekeyParams* __restrict__ rk, u64 which_bit, int S,
                                      u64* __restrict__ out) {
-  constexpr u64 kPer = 8;
-  const u64 stride = (u64)gridDim.x * blockDim.x * kPer;
-  for (u64 q0 = ((u64)blockIdx.x * blockDim.x + threadIdx.x) * kPer; q0 < n; q0 += stride) {
+  constexpr u64 kSpan = 256;
+  const int lane = threadIdx.x & 31;
+  const u64 nwarps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 base = (((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kSpan; base < n; base += nwarps * kSpan) {
+    const u64 q0 = base + lane;
+    if (q0 >= n) continue;
     int lo = 0, hi = count - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (off[mid] <= q0) lo = mid; else hi = mid - 1;
     }
     int p = lo;
-    const u64 q1 = min(q0 + kPer, n);
-    for (u64 q = q0; q < q1; ++q) {
+    const u64 q1 = min(base + kSpan, n);
+    for (u64 q = q0; q < q1; q += 32) {
       while (q >= off[p + 1]) ++p;
       out[q] = ((u64)p << (S + 1)) | which_bit | rekey(keys[q], rk[p]);
     }
@@ -610,8 +617,9 @@ int lnt_batched_contract(int count, const int64_t* dims_host, const uint64_t* a_
   const int sms = sm_count();
   {
     ProfScope prof("batch_compose", s);
-    const u64 ga = std::max<u64>(1, std::min<u64>((C.NA / 8 + 255) / 256, (u64)sms * 16));
-    const u64 gb = std::max<u64>(1, std::min<u64>((C.NB / 8 + 255) / 256, (u64)sms * 16));
+    // one warp per 256 positions, at most 16 CTAs of 8 warps per SM
+    const u64 ga = std::max<u64>(1, std::min<u64>((C.NA + 2047) / 2048, (u64)sms * 16));
+    const u64 gb = std::max<u64>(1, std::min<u64>((C.NB + 2047) / 2048, (u64)sms * 16));
     if (C.NA)
       batch_compose_kernel<<<(unsigned)ga, 256, 0, s>>>((const u64*)a_keys, C.NA,
                                                         reinterpret_cast<const uint64_t*>(w + C.off_aoff), count, rk,
