@@ -78,9 +78,10 @@ __device__ __forceinline__ int find_problem_by_unit(const ProbDesc* prob, int co
 // Column pointers of every problem's A (which == 0) or B (which == 1).
 // Position q enumerates, problem by problem, the n_p + 1 boundaries; position
 // i of problem p fills the pointer entries of the (possibly many empty)
-// columns between entry i-1's column and entry i's.  Each thread takes 8
-// consecutive positions (one binary search for the problem) and fills short
-// ranges itself; a range longer than kLongRun columns (a run of empty columns,
+// columns between entry i-1's column and entry i's.  A warp takes 256
+// consecutive positions, lane-striped (w0 + 32 k + lane: coalesced key loads,
+// adjacent lanes' short ranges adjacent), each lane one binary search for its
+// problem, and each thread fills short ranges itself; a range longer than kLongRun columns (a run of empty columns,
 // common in problems with far more columns than entries) is filled by the
 // whole warp together in coalesced stores, so no thread writes a long run
 // alone.
@@ -91,7 +92,7 @@ __global__ void batch_colptr_kernel(BatchArgs args, int which, const u64* __rest
   const u64 warps = ((u64)gridDim.x * blockDim.x) >> 5;
   const u64 warp_id = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   for (u64 w0 = warp_id * 32 * kPer; w0 < total_pos; w0 += warps * 32 * kPer) {
-    const u64 q0 = w0 + (u64)lane * kPer;
+    const u64 q0 = w0 + (u64)lane;  // lane-striped: positions w0 + 32 k + lane
     int p = 0;
     if (q0 < total_pos) {
       int lo = 0, hi = args.count - 1;
@@ -102,7 +103,7 @@ __global__ void batch_colptr_kernel(BatchArgs args, int which, const u64* __rest
       p = lo;
     }
     for (u64 k = 0; k < kPer; ++k) {
-      const u64 q = q0 + k;
+      const u64 q = q0 + 32 * k;
       long long prev = 0, cur = -1;
       u32 idx = 0;
       u32* ptr = nullptr;
