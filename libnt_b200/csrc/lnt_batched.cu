@@ -64,16 +64,8 @@ struct BatchArgs {
   u32* aptr;
   u32* bptr;
   u64 kmask;  // lattice key bits of the stored keys (the rest is the sort prefix)
+  const u32* uprob;  // the problem of every unit (output column), built at prepare time
 };
-
-__device__ __forceinline__ int find_problem_by_unit(const ProbDesc* prob, int count, u64 u) {
-  int lo = 0, hi = count - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (prob[mid].unit_off <= u) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
 
 // Column pointers of every problem's A (which == 0) or B (which == 1).
 // Position q enumerates, problem by problem, the n_p + 1 boundaries; position
@@ -163,10 +155,8 @@ __global__ void __launch_bounds__(kWarps * 32, 8) batch_spa_kernel(BatchArgs arg
     first = __shfl_sync(0xffffffffu, first, 0);
     if (first >= args.total_units) break;
     const u64 last = min(first + chunk, args.total_units);
-    int p = find_problem_by_unit(args.prob, args.count, first);
     for (u64 u = first; u < last; ++u) {
-      while (u >= args.prob[p].unit_off + args.prob[p].units) ++p;  // chunks may span problems
-      const ProbDesc& P = args.prob[p];
+      const ProbDesc& P = args.prob[args.uprob[u]];  // chunks may span problems
       const u64 lu = u - P.unit_off;  // column id within the problem: col + wB*tab
       const u32* bptr = args.bptr + P.bptr_off;
       const u64 e0 = bptr[lu], e1 = bptr[lu + 1];
@@ -269,7 +259,8 @@ __global__ void batch_coff_kernel(const ProbDesc* __restrict__ prob, int count, 
 
 struct BatchLayout {
   u64 total_units, aptr_len, bptr_len, a_pos, b_pos, c_bound;
-  size_t off_prob, off_apos, off_bpos, off_aptr, off_bptr, off_ucount, off_uoff, off_queue, off_scan, total;
+  size_t off_prob, off_apos, off_bpos, off_aptr, off_bptr, off_ucount, off_uoff, off_queue, off_scan, off_uprob,
+      total;
 };
 
 // interleaved: the operands are read from one array holding A_0 B_0 A_1 B_1 ..
@@ -336,8 +327,20 @@ int batch_layout(int count, const int64_t* dims, const uint64_t* a_off, const ui
   off += 256;
   L->off_scan = off;
   off += align_up(scan::workspace_bytes(L->total_units), 256);
+  L->off_uprob = off;
+  off += align_up(std::max<u64>(L->total_units, 1) * 4, 256);
   L->total = off;
   return LNT_OK;
+}
+
+// The problem of every unit, from the descriptors (units are numbered problem
+// by problem): the product kernels read it instead of searching the
+// descriptors for each column they take.
+std::vector<u32> unit_problems(const std::vector<ProbDesc>& descs, u64 total_units) {
+  std::vector<u32> up(total_units);
+  for (size_t p = 0; p < descs.size(); ++p)
+    std::fill(up.begin() + descs[p].unit_off, up.begin() + descs[p].unit_off + descs[p].units, (u32)p);
+  return up;
 }
 
 struct U64Of {
@@ -514,6 +517,9 @@ int lnt_batched_prepare(int count, const int64_t* dims_host, const uint64_t* a_o
     return LNT_DEVICE_ERROR;
   if (cudaMemcpy(w + L.off_bpos, bpos.data(), bpos.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
     return LNT_DEVICE_ERROR;
+  const std::vector<u32> up = unit_problems(descs, L.total_units);
+  if (!up.empty() && cudaMemcpy(w + L.off_uprob, up.data(), up.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    return LNT_DEVICE_ERROR;
   return LNT_OK;
 }
 
@@ -541,6 +547,7 @@ int lnt_batched_lattice_mult(int count, const int64_t* dims_host, const uint64_t
   args.aptr = reinterpret_cast<u32*>(w + L.off_aptr);
   args.bptr = reinterpret_cast<u32*>(w + L.off_bptr);
   args.kmask = ~0ull;
+  args.uprob = reinterpret_cast<const u32*>(w + L.off_uprob);
   return run_batch_product(args, L, w, count, c_keys, c_vals, d_c_off, s);
 }
 
@@ -579,6 +586,7 @@ int lnt_batched_contract_prepare(int count, const int64_t* dims_host, const uint
     st = make_rekey_params(b_rekey_host ? &b_rekey_host[p] : nullptr, &rk[count + p]);
     if (st != LNT_OK) return st;
   }
+  const std::vector<u32> uprob = unit_problems(descs, L.total_units);
   unsigned char* w = static_cast<unsigned char*>(workspace);
   cudaStream_t s = as_stream(stream);
   // synchronous copies: the host vectors die with this call
@@ -590,11 +598,13 @@ int lnt_batched_contract_prepare(int count, const int64_t* dims_host, const uint
   } copies[] = {{L.off_prob, descs.data(), descs.size() * sizeof(ProbDesc)},
                 {L.off_apos, apos.data(), apos.size() * 8},
                 {L.off_bpos, bpos.data(), bpos.size() * 8},
+                {L.off_uprob, uprob.data(), uprob.size() * 4},
                 {C.off_rk, rk.data(), rk.size() * sizeof(RekeyParams)},
                 {C.off_aoff, a_off_host, (size_t)(count + 1) * 8},
                 {C.off_boff, b_off_host, (size_t)(count + 1) * 8}};
   for (const auto& c : copies)
-    if (cudaMemcpy(w + c.off, c.src, c.bytes, cudaMemcpyHostToDevice) != cudaSuccess) return LNT_DEVICE_ERROR;
+    if (c.bytes && cudaMemcpy(w + c.off, c.src, c.bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+      return LNT_DEVICE_ERROR;
   return LNT_OK;
 }
 
@@ -651,6 +661,7 @@ int lnt_batched_contract(int count, const int64_t* dims_host, const uint64_t* a_
   args.aptr = reinterpret_cast<u32*>(w + C.B.off_aptr);
   args.bptr = reinterpret_cast<u32*>(w + C.B.off_bptr);
   args.kmask = (1ull << C.S) - 1ull;
+  args.uprob = reinterpret_cast<const u32*>(w + C.B.off_uprob);
   return run_batch_product(args, C.B, w, count, c_keys, c_vals, d_c_off, s);
 }
 
