@@ -334,10 +334,11 @@ LNT_API int lnt_contract_attract(const uint64_t* keys, const double* vals, size_
  * *c_capacity bounds the total output.  The reference has no batched form:
  * it is a loop of csc_no_accum calls (SparseLatticeBase.h:1854-1990).
  * Call lnt_batched_prepare once per batch layout (it uploads the descriptor
- * tables into the workspace, synchronously), then lnt_batched_lattice_mult,
- * which only enqueues kernels and memsets on `stream` and can therefore be
- * captured into a CUDA graph and replayed.  Chunk size of the work queue:
- * LNT_BATCH_CHUNK from the environment (default 8). */
+ * tables, including the problem of every output column, into the workspace,
+ * synchronously), then lnt_batched_lattice_mult, which only enqueues kernels
+ * and memsets on `stream` and can therefore be captured into a CUDA graph and
+ * replayed.  Chunk size of the work queue: LNT_BATCH_CHUNK from the
+ * environment, else the autotuned value (1 column). */
 LNT_API int lnt_batched_workspace(int count, const int64_t* dims_host, const uint64_t* a_off_host,
                                   const uint64_t* b_off_host, size_t* bytes, uint64_t* c_capacity);
 LNT_API int lnt_batched_prepare(int count, const int64_t* dims_host, const uint64_t* a_off_host,
