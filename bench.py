@@ -20,6 +20,7 @@ operand pair (no collective on the data path: weak scaling, replicas).
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -716,6 +717,7 @@ def measure_contraction(args):
             hn.copy_(gn, non_blocking=True)
 
     graph_ms, e2e_graph_ms = {}, {}
+    sampler = ClockSampler(torch.cuda.current_device())
     for host_io, res in ((False, graph_ms), (True, e2e_graph_ms)):
         graph_step(host_io)
         torch.cuda.synchronize()
@@ -726,11 +728,12 @@ def measure_contraction(args):
             g.replay()
         torch.cuda.synchronize()
         h0, h1 = _events()
-        h0.record()
-        for _ in range(args.steps):
-            g.replay()
-        h1.record()
-        torch.cuda.synchronize()
+        with sampler if not host_io else contextlib.nullcontext():
+            h0.record()
+            for _ in range(args.steps):
+                g.replay()
+            h1.record()
+            torch.cuda.synchronize()
         res["ms"] = max_over_ranks(h0.elapsed_time(h1) / args.steps, world)
         del g
     assert int(gn.item()) == nc and L.device_status() == 0
@@ -768,7 +771,7 @@ def measure_contraction(args):
     return _line("products/s", prods * world / (ms * 1e-3), ms, args, world, config, {
         "e2e": {"value": prods * world / (e2e_ms * 1e-3), "unit": "products/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 4 * 8 * 10 ** 4, "d2h_bytes_per_step": 16 * nc + 16},
-        "gpu_launches": launches, "cpu_baseline": cpu,
+        "gpu_launches": launches, "cpu_baseline": cpu, "clocks": sampler.summary(),
         "roofline": {"bound": "latency", "note": "about 0.5 MB of data: the step is launch- and latency-bound"},
     })
 
