@@ -140,3 +140,33 @@ def test_sort_merge_graph_capture_matches_oracle(cuda, torch, skewed):
         assert rel_ok(to_host(ov[:m]), ev, ea)
     assert cuda.device_status() == 0
     del g
+
+
+def test_sort_merge_non_power_of_two_full_buckets(cuda, torch):
+    """2 x 3 x 2^24 pairs (a size that is not a power of two): 2^15 buckets of
+    3072 pairs on average, so the bucketed path (7-bit first pass) completes
+    instead of handing the call to the LSD path; the bucket kernel does the
+    work (its time dwarfs the gated fallback's), and the result matches the
+    oracle."""
+    import libnt_b200 as L
+    rng = np.random.default_rng(77)
+    n = 3 << 24
+    ak, av, bk, bv = _operands(rng, n, 0.05)
+    spec = L.RekeySpec.make(DIMS, [0, 1, 2, 3], [3, 2, 1, 0])
+    L.profile_reset()
+    L.profile_enable(True)
+    k, v = cuda.sort_reduce(to_dev(ak, torch), to_dev(av, torch), to_dev(bk, torch), to_dev(bv, torch),
+                            max_key=MAX_KEY, a_rekey=spec)
+    torch.cuda.synchronize()
+    L.profile_enable(False)
+    bucket_ms = L.profile_query("bucket_sort_collect")[0]
+    fallback_ms = L.profile_query("collect_fallback")[0]
+    L.profile_reset()
+    assert cuda.device_status() == 0
+    assert bucket_ms > 10 * fallback_ms, (bucket_ms, fallback_ms)
+    gk, gv = to_host(k, np.uint64), to_host(v)
+    del k, v
+    torch.cuda.empty_cache()
+    ek, ev, ea = _expected(ak, av, bk, bv)
+    np.testing.assert_array_equal(gk, ek)
+    assert rel_ok(gv, ev, ea)
